@@ -1,0 +1,274 @@
+"""Python binding of libbeam_gpu (include/beam_gpu.h) over ctypes.
+
+The product is the C ABI; this module is the thin host-side mirror used by
+the tests, the benchmark and Python callers. It mirrors the reference's
+estimator interface -- the five command-line values of
+``barbie NN NRi UL_k1 LL_k1 BW_k1`` (barbie.c:58-65) plus the constants the
+reference hard-codes (barbie.c:67-84) -- and returns the reference's bin
+arrays (barbie.c:87) as numpy arrays of shape [n_k1bin][n_mtbin][n_mtbin][16].
+
+There is no CPU fallback: loading fails loudly when libbeam_gpu.so is missing,
+and every call that needs a GPU raises BeamError when none is usable.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import weakref
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbeam_gpu.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "beam_gpu.h")
+
+NPOLES = 16
+PREC = {"fp64": 0, "mixed": 1}
+METHOD = {"triangle": 0, "pixel": 1}
+
+BEAM_OK = 0
+BEAM_EINVAL = -1
+BEAM_ENOMEM = -2
+BEAM_EDEVMEM = -3
+BEAM_ECUDA = -4
+BEAM_ETIMEDOUT = -5
+BEAM_EBUSY = -6
+BEAM_EBOUNDS = -7
+BEAM_ENODEV = -8
+BEAM_ENOTFOUND = -9
+
+
+class BeamError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        detail = _lib.beam_gpu_last_error_detail().decode() if _lib is not None else ""
+        msg = _lib.beam_gpu_strerror(code).decode() if _lib is not None else str(code)
+        super().__init__(f"{what}: {msg} ({code}){': ' + detail if detail else ''}")
+
+
+class Cfg(ctypes.Structure):
+    _fields_ = [("NN", ctypes.c_long), ("Nmax", ctypes.c_long), ("Nr", ctypes.c_long),
+                ("UL_k1", ctypes.c_int), ("LL_k1", ctypes.c_int), ("BW_k1", ctypes.c_int),
+                ("n_mtbin", ctypes.c_int), ("LL", ctypes.c_double),
+                ("precision", ctypes.c_int), ("method", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("bs", ctypes.POINTER(ctypes.c_double)), ("norm", ctypes.POINTER(ctypes.c_double)),
+                ("out", ctypes.POINTER(ctypes.c_double)), ("count", ctypes.POINTER(ctypes.c_int64))]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("n_k1bin", ctypes.c_int), ("n_bins", ctypes.c_long), ("n_closed_triplets", ctypes.c_long),
+                ("n_triples", ctypes.c_long), ("n_used_triplets", ctypes.c_long),
+                ("n_fourier_terms", ctypes.c_long), ("n_modes", ctypes.c_long), ("n_planes", ctypes.c_int),
+                ("device_bytes", ctypes.c_size_t), ("vol", ctypes.c_double)]
+
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Every function the public header declares."""
+    with open(HEADER) as fh:
+        text = fh.read()
+    return sorted(set(re.findall(r"^\s*BEAM_API\s+(?:const\s+)?\w+\s*\*?\s*(beam_\w+)\s*\(", text, flags=re.M)))
+
+
+def load() -> ctypes.CDLL:
+    """Load libbeam_gpu.so (built in-tree by ``make -C barbie_b200``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C barbie_b200` (no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+    L.beam_gpu_strerror.argtypes = [ctypes.c_int]
+    L.beam_gpu_strerror.restype = ctypes.c_char_p
+    L.beam_gpu_last_error_detail.argtypes = []
+    L.beam_gpu_last_error_detail.restype = ctypes.c_char_p
+    L.beam_cfg_default.argtypes = [ctypes.POINTER(Cfg), ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.beam_cfg_default.restype = None
+    L.beam_gpu_init.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    L.beam_gpu_destroy.argtypes = [vp]
+    L.beam_gpu_destroy.restype = None
+    L.beam_gpu_plan_create.argtypes = [vp, ctypes.POINTER(Cfg), ctypes.POINTER(vp)]
+    L.beam_gpu_plan_destroy.argtypes = [vp]
+    L.beam_gpu_plan_destroy.restype = None
+    L.beam_gpu_plan_get_info.argtypes = [vp, ctypes.POINTER(PlanInfo)]
+    L.beam_gpu_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Result)]
+    L.beam_gpu_run_batch.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(Result)]
+    L.beam_gpu_closed_rings.argtypes = [vp, dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
+    L.beam_gpu_plane_rings.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int, vp, ctypes.c_int]
+    L.beam_gpu_triangle_sums.argtypes = [vp, vp, ctypes.c_int, dp]
+    L.beam_gpu_stream.argtypes = [vp]
+    L.beam_gpu_stream.restype = vp
+    L.beam_gpu_plan_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+    L.beam_gpu_plan_last_timings.restype = ctypes.c_int
+    for name in ("beam_gpu_init", "beam_gpu_plan_create", "beam_gpu_plan_get_info", "beam_gpu_run",
+                 "beam_gpu_run_batch", "beam_gpu_closed_rings", "beam_gpu_plane_rings", "beam_gpu_triangle_sums"):
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != BEAM_OK:
+        raise BeamError(rc, what)
+
+
+def _ptr(a):
+    """(address, on_device) of a C-contiguous float64 numpy array or torch tensor."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags.c_contiguous:
+            raise TypeError("expected a C-contiguous float64 array")
+        return a.ctypes.data, 0
+    if hasattr(a, "data_ptr"):  # torch tensor
+        import torch
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise TypeError("expected a contiguous float64 tensor")
+        return a.data_ptr(), 1 if a.is_cuda else 0
+    raise TypeError(f"unsupported buffer type {type(a)}")
+
+
+class Context:
+    """One CUDA device and stream (beam_gpu_init)."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = ctypes.c_void_p()
+        _check(L.beam_gpu_init(device, ctypes.byref(h)), "beam_gpu_init")
+        self._h = h
+        self.device = device
+        self._plans = weakref.WeakSet()
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t the library launches on (address)."""
+        return _lib.beam_gpu_stream(self._h) or 0
+
+    def close(self) -> None:
+        """Destroy the context; plans made on it are destroyed first."""
+        if getattr(self, "_h", None):
+            for plan in list(self._plans):
+                plan.close()
+            _lib.beam_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """Estimator plan for one configuration (beam_gpu_plan_create)."""
+
+    def __init__(self, ctx: Context, NN: int, UL_k1: int, LL_k1: int, BW_k1: int, *, Nmax: int = 100,
+                 Nr: int = 40, n_mtbin: int = 5, LL: float = 1.0, precision: str = "fp64",
+                 method: str = "triangle"):
+        L = load()
+        cfg = Cfg()
+        L.beam_cfg_default(ctypes.byref(cfg), NN, UL_k1, LL_k1, BW_k1)
+        cfg.Nmax, cfg.Nr, cfg.n_mtbin, cfg.LL = Nmax, Nr, n_mtbin, LL
+        cfg.precision, cfg.method = PREC[precision], METHOD[method]
+        h = ctypes.c_void_p()
+        _check(L.beam_gpu_plan_create(ctx._h, ctypes.byref(cfg), ctypes.byref(h)), "beam_gpu_plan_create")
+        self._h, self.ctx, self.cfg = h, ctx, cfg
+        ctx._plans.add(self)
+        info = PlanInfo()
+        _check(L.beam_gpu_plan_get_info(h, ctypes.byref(info)), "beam_gpu_plan_get_info")
+        self.info = {k: getattr(info, k) for k, _ in PlanInfo._fields_}
+        self.n_k1bin = info.n_k1bin
+        self.shape = (info.n_k1bin, n_mtbin, n_mtbin, NPOLES)
+        self.NN = NN
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.beam_gpu_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _result(self):
+        bs, nm, out = (np.zeros(self.shape) for _ in range(3))
+        cnt = np.zeros(self.shape[:3], dtype=np.int64)
+        res = Result(bs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     nm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        return res, dict(bs=bs, norm=nm, out=out, count=cnt)
+
+    def run(self, r2c) -> dict:
+        """One bispectrum of an r2c buffer (numpy host array or torch CUDA tensor)."""
+        addr, dev = _ptr(r2c)
+        self._check_size(r2c)
+        res, arrays = self._result()
+        _check(_lib.beam_gpu_run(self._h, addr, dev, ctypes.byref(res)), "beam_gpu_run")
+        return arrays
+
+    def run_batch(self, fields: list) -> list[dict]:
+        """Several realizations (host numpy arrays) through beam_gpu_run_batch."""
+        addrs = (ctypes.c_void_p * len(fields))()
+        results = (Result * len(fields))()
+        out = []
+        for k, f in enumerate(fields):
+            a, dev = _ptr(f)
+            if dev:
+                raise TypeError("run_batch takes host arrays")
+            self._check_size(f)
+            addrs[k] = a
+            results[k], arrays = self._result()
+            out.append(arrays)
+        _check(_lib.beam_gpu_run_batch(self._h, addrs, len(fields), results), "beam_gpu_run_batch")
+        return out
+
+    def triangle_sums(self, r2c) -> np.ndarray:
+        """B per accepted triangle in the reference's loop order."""
+        addr, dev = _ptr(r2c)
+        self._check_size(r2c)
+        B = np.zeros(max(1, self.info["n_triples"]))
+        _check(_lib.beam_gpu_triangle_sums(self._h, addr, dev, B.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+               "beam_gpu_triangle_sums")
+        return B[: self.info["n_triples"]]
+
+    def closed_rings(self) -> np.ndarray:
+        """calCR records {r1, r2, r3, Num = NN^2 * count}."""
+        n = ctypes.c_long(0)
+        cap = self.info["n_closed_triplets"]
+        out = np.zeros((max(cap, 1), 4))
+        _check(_lib.beam_gpu_closed_rings(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), cap,
+                                          ctypes.byref(n)), "beam_gpu_closed_rings")
+        return out[: n.value]
+
+    def plane_rings(self, r2c, planes, rings) -> np.ndarray:
+        """Df transforms -> complex128[n][NN][NN] (host)."""
+        addr, dev = _ptr(r2c)
+        self._check_size(r2c)
+        planes = np.ascontiguousarray(planes, dtype=np.int32)
+        rings = np.ascontiguousarray(rings, dtype=np.int32)
+        n = len(planes)
+        out = np.zeros((n, self.NN, self.NN), dtype=np.complex128)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _check(_lib.beam_gpu_plane_rings(self._h, addr, dev, planes.ctypes.data_as(ip), rings.ctypes.data_as(ip),
+                                         n, out.ctypes.data, 0), "beam_gpu_plane_rings")
+        return out
+
+    def last_timings(self) -> dict:
+        """Device milliseconds of the stages of the last run (CUDA events)."""
+        ms = (ctypes.c_float * 4)()
+        _check(_lib.beam_gpu_plan_last_timings(self._h, ms, 4), "beam_gpu_plan_last_timings")
+        return dict(upload=ms[0], triangle=ms[1], reduce=ms[2], epilogue=ms[3])
+
+    def _check_size(self, r2c) -> None:
+        NN = self.NN
+        if tuple(r2c.shape) not in ((NN, NN, NN + 2), (NN * NN * (NN + 2),)):
+            raise ValueError(f"r2c buffer must be [{NN}][{NN}][{NN + 2}] float64")

@@ -1,0 +1,165 @@
+/* Drop-in for the reference estimator program `barbie NN NRi UL_k1 LL_k1 BW_k1`
+ * (barbie.c:26-399 of sukhdeepsinghgill/BARBIE), running the hot path on a
+ * B200 through libbeam_gpu.
+ *
+ * Same command line, same input and outputs as the reference:
+ *   input   ./field_N<NN>_R<NRi>.txt   raw native doubles, r2c layout [NN][NN][NN+2]
+ *   output  ResFiles_N<NN>/BS_test_ii<ii>_N<NN>_R<NRi>.txt, ii = 0..15, rows
+ *           "%d\t%d\t%d\t%e\t%e\t%f\n" = k1 bin, t bin, mu bin, multipole,
+ *           analytic column, normalisation/NN^2, for bins whose monopole
+ *           normalisation exceeds 0.1 (barbie.c:383-397)
+ *           ResFiles_N<NN>/time_<NN>_R<NRi>.txt  ("Total time ...")
+ * The reference's hard-coded constants (barbie.c:67-84) are the defaults;
+ * optional environment overrides, all unset by default:
+ *   BEAM_NMAX, BEAM_NR        planes and rings (100, 40)
+ *   BEAM_PRECISION            fp64 (default) or mixed
+ *   BEAM_METHOD               triangle (default) or pixel
+ *   BEAM_DEVICE               CUDA device ordinal (0)
+ *   BEAM_PRINT_DIGITS         significant digits of columns 4-6 (default: the
+ *                             reference's %e / %f)
+ * Differences from the reference, all on paths where it is undefined: the
+ * analytic-comparison column 5 is written from a zero-initialised accumulator
+ * (the reference never initialises bin_Biana, barbie.c:87,203-210), a missing
+ * ResFiles_N<NN> directory is created, and invalid arguments or an unreadable
+ * field file are reported instead of crashing. */
+#include <errno.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <time.h>
+
+#include "beam_gpu.h"
+
+static long env_long(const char *name, long fallback) {
+  const char *v = getenv(name);
+  return (v && *v) ? strtol(v, NULL, 10) : fallback;
+}
+
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static int fail(const char *what, int rc) {
+  fprintf(stderr, "barbie: %s: %s (%s)\n", what, beam_gpu_strerror(rc), beam_gpu_last_error_detail());
+  return 1;
+}
+
+int main(int argc, char *argv[]) {
+  long NN;
+  int NRi, UL_k1, LL_k1, BW_k1;
+  if (argc != 6) { /* barbie.c:58-60 */
+    printf("Usage: %s NN(384) NRi(1) UL_k1(Nmax) LL_k1(Nmax-10) BW_k1(1)\n", argv[0]);
+    return 1;
+  }
+  if (sscanf(argv[1], "%ld", &NN) != 1 || sscanf(argv[2], "%d", &NRi) != 1 || sscanf(argv[3], "%d", &UL_k1) != 1 ||
+      sscanf(argv[4], "%d", &LL_k1) != 1 || sscanf(argv[5], "%d", &BW_k1) != 1) {
+    fprintf(stderr, "barbie: arguments must be integers\n");
+    return 1;
+  }
+  printf("\n Calculating BS Multipoles for Realization(NRi) = %d and Grids(NN) = %ld\n", NRi, NN);
+
+  beam_cfg cfg;
+  beam_cfg_default(&cfg, NN, UL_k1, LL_k1, BW_k1);
+  cfg.Nmax = env_long("BEAM_NMAX", cfg.Nmax);
+  cfg.Nr = env_long("BEAM_NR", cfg.Nr);
+  const char *prec = getenv("BEAM_PRECISION");
+  if (prec && strcmp(prec, "mixed") == 0) cfg.precision = BEAM_PREC_MIXED;
+  const char *meth = getenv("BEAM_METHOD");
+  if (meth && strcmp(meth, "pixel") == 0) cfg.method = BEAM_METHOD_PIXEL;
+  int digits = (int)env_long("BEAM_PRINT_DIGITS", 0);
+
+  /* input field, barbie.c:176-185 (one read instead of one fread per double) */
+  char path[256];
+  snprintf(path, sizeof(path), "field_N%ld_R%d.txt", NN, NRi);
+  size_t n = (size_t)NN * (size_t)NN * (size_t)(NN + 2);
+  double *field = (double *)malloc(sizeof(double) * n);
+  if (!field) {
+    fprintf(stderr, "barbie: cannot allocate %zu bytes for the field\n", sizeof(double) * n);
+    return 1;
+  }
+  FILE *fp = fopen(path, "rb");
+  if (!fp) {
+    fprintf(stderr, "barbie: cannot open %s: %s\n", path, strerror(errno));
+    return 1;
+  }
+  size_t got = fread(field, sizeof(double), n, fp);
+  fclose(fp);
+  if (got != n) {
+    fprintf(stderr, "barbie: %s holds %zu doubles, expected %zu\n", path, got, n);
+    return 1;
+  }
+
+  double t0 = now_s();
+  beam_gpu_ctx *ctx = NULL;
+  beam_gpu_plan *plan = NULL;
+  int rc = beam_gpu_init((int)env_long("BEAM_DEVICE", 0), &ctx);
+  if (rc) return fail("device set-up", rc);
+  rc = beam_gpu_plan_create(ctx, &cfg, &plan);
+  if (rc) return fail("plan (ring geometry, closed triplets, triangles)", rc);
+  beam_plan_info info;
+  beam_gpu_plan_get_info(plan, &info);
+  printf("\n All parameters are with me including mu-t bins=%d, k1 bins=%d  !!\n", cfg.n_mtbin, info.n_k1bin);
+  printf(" closed ring triplets %ld, accepted triangles %ld, plan %.3f s\n", info.n_closed_triplets,
+         info.n_triples, now_s() - t0);
+
+  size_t nb = (size_t)info.n_bins;
+  double *bs = (double *)calloc(nb * BEAM_NPOLES, sizeof(double));
+  double *norm = (double *)calloc(nb * BEAM_NPOLES, sizeof(double));
+  double *out = (double *)calloc(nb * BEAM_NPOLES, sizeof(double));
+  int64_t *count = (int64_t *)calloc(nb ? nb : 1, sizeof(int64_t));
+  if (!bs || !norm || !out || !count) {
+    fprintf(stderr, "barbie: out of host memory\n");
+    return 1;
+  }
+  beam_result res = {bs, norm, out, count};
+  double t1 = now_s();
+  rc = beam_gpu_run(plan, field, 0, &res);
+  if (rc) return fail("bispectrum", rc);
+  double loop_time = now_s() - t1;
+  printf("Total time %f\n", loop_time);
+
+  char dir[64];
+  snprintf(dir, sizeof(dir), "ResFiles_N%ld", NN);
+  if (mkdir(dir, 0755) != 0 && errno != EEXIST) {
+    fprintf(stderr, "barbie: cannot create %s: %s\n", dir, strerror(errno));
+    return 1;
+  }
+  snprintf(path, sizeof(path), "%s/time_%ld_R%d.txt", dir, NN, NRi);
+  fp = fopen(path, "w");
+  if (fp) {
+    fprintf(fp, "Total time %f\n", loop_time);
+    fclose(fp);
+  }
+  const int nm = cfg.n_mtbin;
+  for (int ii = 0; ii < BEAM_NPOLES; ++ii) { /* barbie.c:383-397 */
+    snprintf(path, sizeof(path), "%s/BS_test_ii%d_N%ld_R%d.txt", dir, ii, NN, NRi);
+    fp = fopen(path, "w");
+    if (!fp) {
+      fprintf(stderr, "barbie: cannot write %s: %s\n", path, strerror(errno));
+      return 1;
+    }
+    for (int i = 0; i < info.n_k1bin; i++)
+      for (int j = 0; j < nm; j++)
+        for (int l = 0; l < nm; l++) {
+          size_t b = ((size_t)i * nm + j) * nm + l;
+          double nrm = norm[b * BEAM_NPOLES + ii];
+          double val = out[b * BEAM_NPOLES + ii];
+          double ana = 0.0 / nrm; /* zero-initialised analytic accumulator over its normalisation */
+          if (norm[b * BEAM_NPOLES + 0] > .1) {
+            if (digits > 0)
+              fprintf(fp, "%d\t%d\t%d\t%.*e\t%.*e\t%.*e\n", i, j, l, digits - 1, val, digits - 1, ana, digits - 1,
+                      nrm / ((double)NN * NN * 1.));
+            else
+              fprintf(fp, "%d\t%d\t%d\t%e\t%e\t%f\n", i, j, l, val, ana, nrm / ((double)NN * NN * 1.));
+          }
+        }
+    fclose(fp);
+  }
+  beam_gpu_plan_destroy(plan);
+  beam_gpu_destroy(ctx);
+  free(field); free(bs); free(norm); free(out); free(count);
+  return 0;
+}

@@ -1,0 +1,169 @@
+/* libbeam_gpu: B200 (sm_100a) implementation of the BEAM redshift-space
+ * bispectrum estimator hot path of sukhdeepsinghgill/BARBIE, behind a plain C ABI.
+ *
+ * The reference has no plugin or FFI layer: its boundary is the program
+ * `barbie NN NRi UL_k1 LL_k1 BW_k1` (barbie.c:26-399) and its files. The C host
+ * drop-in (barbie_b200/host/barbie_main.c) keeps that command line and those
+ * files and calls the entry points below, each of which replaces one stage of
+ * the reference (cited per function).
+ *
+ * Conventions: every call returns BEAM_OK (0) or a negative BEAM_E* code and
+ * never exits the process; the caller owns host buffers, the library owns
+ * device state; a plan is not re-entrant (one host thread per plan at a time);
+ * device waits are bounded and report BEAM_ETIMEDOUT.
+ *
+ * Array layouts (all row-major, native-endian):
+ *   r2c    double[NN][NN][NN+2]: the FFTW in-place r2c buffer of Delta(k),
+ *          i.e. complex128[NN][NN][NN/2+1] with the last axis the line of sight
+ *          (barbie.c:176-185, field_N<NN>_R<NRi>.txt).
+ *   bins   double[n_k1bin][n_mtbin][n_mtbin][16] (barbie.c:87), with
+ *          n_k1bin = (UL_k1-LL_k1)/BW_k1 (barbie.c:84).
+ */
+#ifndef BEAM_GPU_H
+#define BEAM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BEAM_API __attribute__((visibility("default")))
+#else
+#define BEAM_API
+#endif
+
+#define BEAM_NPOLES 16
+
+/* error codes */
+#define BEAM_OK 0
+#define BEAM_EINVAL (-1)     /* invalid configuration or argument */
+#define BEAM_ENOMEM (-2)     /* host allocation failed */
+#define BEAM_EDEVMEM (-3)    /* device allocation failed or footprint refused */
+#define BEAM_ECUDA (-4)      /* a CUDA runtime call failed */
+#define BEAM_ETIMEDOUT (-5)  /* a bounded device wait gave up */
+#define BEAM_EBUSY (-6)      /* queue full / slot not available */
+#define BEAM_EBOUNDS (-7)    /* a triangle's bin index falls outside the bin arrays */
+#define BEAM_ENODEV (-8)     /* no usable CUDA device */
+#define BEAM_ENOTFOUND (-9)  /* unknown job id */
+
+/* precision of the triple-product sums */
+#define BEAM_PREC_FP64 0  /* FP64 throughout (parity path, 1e-10 of the reference) */
+#define BEAM_PREC_MIXED 1 /* FP32 mode data and products, FP32 chunk sums, FP64 across chunks */
+
+/* how the per-triangle sums B = sum_x Re(F1 F2 F3) are formed */
+#define BEAM_METHOD_TRIANGLE 0 /* over closed in-plane Fourier triangles (default) */
+#define BEAM_METHOD_PIXEL 1    /* over the NN^2 pixels of the per-(plane,ring) IFFTs, as the reference */
+
+typedef struct beam_gpu_ctx beam_gpu_ctx;
+typedef struct beam_gpu_plan beam_gpu_plan;
+
+/* Estimator configuration. The reference hard-codes all but the first three
+ * command-line values in barbie.c:67-84: Nmax=100, Nr=40, n_mtbin=5, LL=1. */
+typedef struct beam_cfg {
+  long NN;        /* grid size (even) */
+  long Nmax;      /* number of line-of-sight planes (barbie.c:71) */
+  long Nr;        /* number of rings, a multiple of 10 (barbie.c:72,111-114) */
+  int UL_k1;      /* upper k1 limit, grid units (argv[3]) */
+  int LL_k1;      /* lower k1 limit (argv[4]) */
+  int BW_k1;      /* k1 bin width (argv[5]) */
+  int n_mtbin;    /* mu and t bins on [0.5,1] (barbie.c:84) */
+  double LL;      /* cell size for vol=(NN*LL)^3 (barbie.c:67,76) */
+  int precision;  /* BEAM_PREC_* */
+  int method;     /* BEAM_METHOD_* */
+} beam_cfg;
+
+/* Fill cfg with the reference's defaults for the given command-line values. */
+BEAM_API void beam_cfg_default(beam_cfg *cfg, long NN, int UL_k1, int LL_k1, int BW_k1);
+
+/* Estimator output; any pointer may be NULL. */
+typedef struct beam_result {
+  double *bs;     /* bins: sum of B*bs[ii]           (bin_BS_real, barbie.c:360) */
+  double *norm;   /* bins: sum of Num*norm[ii]       (bin_normalization, barbie.c:362) */
+  double *out;    /* bins: bs/(vol*norm)             (the value barbie.c:390-393 prints) */
+  int64_t *count; /* [n_k1bin][n_mtbin][n_mtbin]: exact number of closed triangles summed
+                     into the bin (those with B != 0); norm[..][0] = NN^2 * count */
+} beam_result;
+
+typedef struct beam_plan_info {
+  int n_k1bin;            /* bins along k1 */
+  long n_bins;            /* n_k1bin * n_mtbin^2 */
+  long n_closed_triplets; /* ring triplets passing the closure test (calCR's rcount) */
+  long n_triples;         /* accepted (p1, ring triplet, p2) triangles of the loop */
+  long n_used_triplets;   /* distinct ring triplets among them */
+  long n_fourier_terms;   /* sum over accepted triangles of their in-plane triangle counts */
+  long n_modes;           /* ring modes on the planes in use */
+  int n_planes;           /* planes |p| in use (0..n_planes-1) */
+  size_t device_bytes;    /* device memory held by the plan (tables + per-run buffers) */
+  double vol;             /* (NN*LL)^3 */
+} beam_plan_info;
+
+/* Library / device setup. Replaces the fftw_init_threads / plan_with_nthreads
+ * set-up of barbie.c:151-153. */
+BEAM_API int beam_gpu_init(int device, beam_gpu_ctx **out);
+BEAM_API void beam_gpu_destroy(beam_gpu_ctx *ctx);
+
+/* Geometry plan: ring edges and masks (barbie.c:110-148), closed ring triplets
+ * with exact triangle counts (calCR, funcs.c:328-424, in place of the
+ * closed_rings_<NN> disk cache, barbie.c:161-164), and the accepted triangles of
+ * the loop with their K1/T/MU/px/pz and bins (barbie.c:247-298,343-345). The
+ * plan is independent of the field and is reused for every realization. */
+BEAM_API int beam_gpu_plan_create(beam_gpu_ctx *ctx, const beam_cfg *cfg, beam_gpu_plan **out);
+BEAM_API void beam_gpu_plan_destroy(beam_gpu_plan *plan);
+BEAM_API int beam_gpu_plan_get_info(const beam_gpu_plan *plan, beam_plan_info *info);
+
+/* One bispectrum: plane-ring transforms (wrapid_fast/Df, funcs.c:537-566,88-109,
+ * held on the device instead of the disk cache), the triple products of the loop
+ * (barbie.c:315-337), binning and cal_coeff weights (barbie.c:343-363,
+ * funcs.c:708-745) and the normalisation (barbie.c:383-392).
+ * r2c: double[NN][NN][NN+2], in host memory (r2c_on_device=0, pageable or
+ * pinned) or device memory (r2c_on_device=1). Results go to host memory. */
+BEAM_API int beam_gpu_run(beam_gpu_plan *plan, const double *r2c, int r2c_on_device, beam_result *res);
+
+/* Several realizations of one plan in one call: the per-realization mode data
+ * and partial sums stay on the device and all realizations' triangle sums run
+ * in one launch sequence (captured once into a CUDA graph and replayed).
+ * r2c[i] are host buffers; res[i] receives realization i. */
+BEAM_API int beam_gpu_run_batch(beam_gpu_plan *plan, const double *const *r2c, int n, beam_result *res);
+
+/* calCR (funcs.c:328-424): closed ring triplets in the reference's order as
+ * records {r1, r2, r3, Num} with Num = NN^2 * (exact triangle count) -- the
+ * quantity the reference computes by FFT with round-off. Writes up to cap
+ * records; *rcount receives the total. */
+BEAM_API int beam_gpu_closed_rings(beam_gpu_plan *plan, double *rings4, long cap, long *rcount);
+
+/* Df / wrapid_fast (funcs.c:88-109,537-566): for each of n (plane, ring) pairs
+ * (0 <= plane < Nmax, 0 <= ring < Nr) the unnormalised backward 2D DFT of the
+ * ring-masked plane, k_perp=0 zeroed on plane 0, as complex128[NN][NN] written
+ * to out + k*2*NN*NN (host memory unless out_on_device). Runs on the GPU with
+ * the library's FFT kernels in FP64. */
+BEAM_API int beam_gpu_plane_rings(beam_gpu_plan *plan, const double *r2c, int r2c_on_device,
+                         const int *planes, const int *rings, int n, double *out, int out_on_device);
+
+/* Per-triangle sums B (barbie.c:326-337, the value added at :360 before the bs
+ * weight) for all accepted triangles in loop order, written to B (host, n_triples
+ * doubles). The plan's method and precision apply. */
+BEAM_API int beam_gpu_triangle_sums(beam_gpu_plan *plan, const double *r2c, int r2c_on_device, double *B);
+
+/* The cudaStream_t (as void*) the context launches all its work on, for
+ * callers that order their own work after it or record events on it. */
+BEAM_API void *beam_gpu_stream(beam_gpu_ctx *ctx);
+
+/* Device time of the stages of the plan's last run/triangle_sums call, in
+ * milliseconds, measured with CUDA events on the context's stream:
+ * [0] mode upload + gather, [1] triangle sums (the dominant kernel),
+ * [2] split reduction, [3] bins epilogue. Writes min(n, 4) values. */
+BEAM_API int beam_gpu_plan_last_timings(const beam_gpu_plan *plan, float *ms, int n);
+
+/* Human-readable text for an error code. */
+BEAM_API const char *beam_gpu_strerror(int code);
+
+/* Details of the last error on this thread (CUDA error string etc.). */
+BEAM_API const char *beam_gpu_last_error_detail(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

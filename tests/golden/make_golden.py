@@ -1,0 +1,94 @@
+"""Generate the golden fixtures of the parity tests from the reference itself.
+
+Each case writes a seeded synthetic field (barbie_b200.synth) in the reference's
+input format, runs the reference estimator program oracle/_ref/barbie_ref --
+compiled by oracle/Makefile from the reference's own barbie.c/funcs.c with the
+FFTW-API shim, printing %.17e instead of %e/%f -- in a scratch directory, and
+stores its 16 output files as one small .npz:
+
+  rows   float64[n, 6]: ii, k1 bin, t bin, mu bin, multipole value (column 4),
+         normalisation / NN^2 (column 6)
+  field_sha256, and the configuration.
+
+Column 5 (the analytic accumulator) is not stored: the reference never
+initialises it (barbie.c:87,203-210).
+
+Usage: python tests/golden/make_golden.py [case ...]     (default: all cases)
+Needs the reference sources (to build oracle/_ref) -- run where they exist.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from barbie_b200.synth import realization_seed, synth_field, write_field  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "barbie_ref")
+
+# name: (NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, realization)
+CASES = {
+    # BASELINE config 1 (CPU-runnable): NN=64, Nmax=16, Nr=10, bins 1..11 width 1
+    "nn64_cfg1": (64, 16, 10, 11, 1, 1, 1),
+    # same geometry, other realization, wider bins and an offset k1 range
+    "nn64_bw2": (64, 16, 10, 13, 3, 2, 2),
+    # radix-3 grid, 20 rings in two blocks of widths 1 and 2
+    "nn96_r20": (96, 32, 20, 21, 1, 1, 3),
+    # NN=256, Nmax=64, Nr=30, bins 1..31 width 1
+    "nn256_cfg2": (256, 64, 30, 31, 1, 1, 1),
+}
+
+
+def run_case(name: str, scratch: str) -> str:
+    NN, Nmax, Nr, UL, LL, BW, r = CASES[name]
+    work = os.path.join(scratch, name)
+    shutil.rmtree(work, ignore_errors=True)
+    os.makedirs(os.path.join(work, f"ResFiles_N{NN}", "data_files"))
+    field = synth_field(NN, realization_seed(r))
+    write_field(os.path.join(work, f"field_N{NN}_R{r}.txt"), field)
+    env = dict(os.environ, BEAM_REF_NMAX=str(Nmax), BEAM_REF_NR=str(Nr))
+    t = time.time()
+    with open(os.path.join(work, "run.log"), "w") as log:
+        subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {REF_BIN} {NN} {r} {UL} {LL} {BW}"],
+                       cwd=work, env=env, stdout=log, stderr=subprocess.STDOUT, check=True)
+    rows = []
+    for ii in range(16):
+        path = os.path.join(work, f"ResFiles_N{NN}", f"BS_test_ii{ii}_N{NN}_R{r}.txt")
+        with open(path) as fh:
+            for line in fh:
+                f = line.split()
+                rows.append([ii, int(f[0]), int(f[1]), int(f[2]), float(f[3]), float(f[5])])
+    out = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(out, rows=np.array(rows, dtype=np.float64),
+                        field_sha256=hashlib.sha256(field.tobytes()).hexdigest(),
+                        config=np.array([NN, Nmax, Nr, UL, LL, BW, r], dtype=np.int64))
+    shutil.rmtree(work, ignore_errors=True)
+    print(f"{name}: {len(rows)} rows in {time.time() - t:.1f} s -> {out}")
+    return out
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("cases", nargs="*", default=list(CASES))
+    ap.add_argument("--scratch", default=os.path.join(HERE, ".scratch"))
+    args = ap.parse_args()
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
+    if not os.path.exists(REF_BIN):
+        sys.exit("oracle/_ref/barbie_ref is missing: the reference sources are needed to build it")
+    for c in args.cases:
+        run_case(c, args.scratch)
+    shutil.rmtree(args.scratch, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()
