@@ -75,9 +75,14 @@ int beam_gpu_init(int device, beam_gpu_ctx **out) {
   c->num_sms = prop.multiProcessorCount;
   c->smem_optin = prop.sharedMemPerBlockOptin;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  for (int k = 0; k < TRI_WARPS && e == cudaSuccess; ++k) {
+    e = cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     set_detail(cudaGetErrorString(e));
-    delete c;
+    beam_gpu_destroy(c);
     return BEAM_ECUDA;
   }
   *out = c;
@@ -87,6 +92,11 @@ int beam_gpu_init(int device, beam_gpu_ctx **out) {
 void beam_gpu_destroy(beam_gpu_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  for (int k = 0; k < TRI_WARPS; ++k) {
+    if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
+    if (ctx->join[k]) cudaEventDestroy(ctx->join[k]);
+  }
+  if (ctx->fork) cudaEventDestroy(ctx->fork);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }

@@ -38,27 +38,67 @@ void set_detail(const std::string &s);
 enum : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BAD_INDEX = 2 };
 
 // Threads per triangle-sum CTA and in-plane triangles staged per pipeline stage.
-constexpr int TRI_THREADS = 256;
-constexpr int TRI_CHUNK = 16;  // upper bound; the launch may stage fewer
-constexpr int TRI_MAX_SLOTS = 16;  // combos per thread
+// Triangle-sum decomposition. Each warp owns a tile of TRI_P1 planes p1 x 32
+// planes p3 (one p3 per lane, p2 = -p1-p3) of one ring triplet's accepted
+// (p1, p2) "combos"; a CTA holds up to TRI_WARPS tiles of the same triplet.
+// The triplet's in-plane triangles are listed k2-major, so consecutive
+// triangles sharing k2 form a run; runs are cut into pieces of at most
+// TRI_CHUNK triangles and whole pieces are packed into chunks of at most
+// TRI_CHUNK triangles, one pipeline stage each.
+constexpr int TRI_WARPS = 7;   // most tiles per CTA (one consumer warp each, plus one producer warp)
+constexpr int TRI_P1 = 8;      // planes p1 per thread
+constexpr int TRI_CHUNK = 16;  // in-plane triangles per stage
+constexpr int TRI_PIECES = 4;  // pieces per stage
+constexpr int TRI_STAGES = 3;  // pipeline depth
+constexpr int TRI_PAD = 8;     // zero columns on each side of a mode row (>= TRI_P1 - 1)
 
-// One unit of triangle-sum work: combos [c0, c1) of one used ring triplet over
-// its in-plane triangles [t0, t1). Rows staged per triangle are the columns
-// [p1lo, p1lo+L1), [p2lo, p2lo+L2), [p3lo, p3lo+L3) of the signed-plane mode
-// rows of rings r1, r2, r3 (column of plane q is q + Q - 1).
+struct TriTile {
+  int p1_0, p3_0;  // planes p1_0 + a (a < TRI_P1) and p3_0 + lane
+};
+
+struct TriChunk {
+  long long t0;  // first in-plane triangle (global list index)
+  int pc0;       // first piece in the global piece table
+  int packed;    // nt (bits 0-4), npc (bits 5-7), piece lengths (5 bits each from bit 8)
+};
+// fields of TriChunk::packed / TriDesc::packed
+__host__ __device__ inline int chunk_nt(int packed) { return packed & 31; }
+__host__ __device__ inline int chunk_npc(int packed) { return (packed >> 5) & 7; }
+__host__ __device__ inline int chunk_len(int packed, int piece) { return (packed >> (8 + 5 * piece)) & 31; }
+__host__ __device__ inline int chunk_pack(int nt, int npc, int lens) { return nt | (npc << 5) | (lens << 8); }
+
+// What the kernel reads per chunk: the layout and, for each triangle and
+// piece, the row (mode index within its ring) to stage -- one independent
+// load per producer lane.
+struct TriDesc {
+  uint16_t xz[TRI_CHUNK][2];  // triangle j: k1 (ring r1) and k3 (ring r3)
+  uint16_t y[TRI_PIECES];     // piece j: k2 (ring r2)
+  int packed;                 // as TriChunk::packed
+  int pad;
+};
+static_assert(sizeof(TriDesc) % 16 == 0 && TRI_CHUNK <= 31 && TRI_PIECES <= 4, "TriDesc layout");
+constexpr int TRI_TAU_MAX = 512;  // most in-plane triangles walked by one CTA
+
+// One CTA of triangle-sum work: tiles [tile0, tile0 + ntiles) of ring triplet u
+// over chunks [ch0, ch1) (the triplet's split `split`). Rows staged per chunk
+// are columns [colx, colx+Lx) of ring r1's mode rows (one per triangle),
+// [colz, colz+Lz) of ring r3's (one per triangle) and [coly, coly+Ly) of ring
+// r2's (one per piece); the column of plane q is q + Q - 1.
 struct TriItem {
-  int u;               // used ring triplet
-  int split;           // index of this triangle range among the triplet's splits
-  int c0, c1;          // combos (global combo indices)
-  long long t0, t1;    // in-plane triangles (global triangle-list indices)
-  int m1, m2, m3;      // first mode of rings r1, r2, r3 in the mode table
-  int p1lo, L1, p2lo, L2, p3lo, L3;
+  int u, split;
+  int ch0, ch1;
+  int tile0, ntiles;
+  int m1, m2, m3;  // first mode of rings r1, r2, r3 in the mode table
+  int colx, Lx, colz, Lz, coly, Ly;
 };
 
 // Device-side tables and buffers of a plan.
 struct DevPlan {
   // ring modes on the planes in use
-  int n_modes = 0, Q = 0, W = 0;  // modes, planes |p| < Q in use, signed-plane row width 2Q-1
+  // A mode's row holds planes q = -(Q-1)..Q-1 at columns colbase + q, with
+  // TRI_PAD zero columns on either side (reads of neighbouring planes by
+  // threads whose combos are not accepted stay inside the row).
+  int n_modes = 0, Q = 0, W = 0, colbase = 0;
   int16_t *mode_ij = nullptr;     // [n_modes][2] grid indices (i, j)
   int32_t *mode_neg = nullptr;    // [n_modes] mode at -k
   int16_t *ringmap = nullptr;     // [NN*NN] ring of each pixel or -1
@@ -69,19 +109,25 @@ struct DevPlan {
   // accepted triangles grouped by ring triplet ("combos": plane pairs p1, p2)
   int n_used = 0;
   long long n_combo = 0;
-  int32_t *combo_p1 = nullptr, *combo_p2 = nullptr;  // [n_combo]
   int32_t *combo_u = nullptr;     // [n_combo] used ring triplet
   int32_t *combo_out = nullptr;   // [n_combo] bin-order position of the triangle
   int32_t *u_cfirst = nullptr;    // [n_used] first combo
   int32_t *u_ncombo = nullptr;    // [n_used]
   int32_t *u_nsplit = nullptr;    // [n_used] triangle-range splits
   long long *u_part = nullptr;    // [n_used] first partial-sum slot (split-major)
+  int n_tiles = 0;
+  TriTile *tiles = nullptr;       // [n_tiles]
+  int32_t *tile_combo = nullptr;  // [n_tiles][TRI_P1][32] combo id or -1
+  long long n_chunks = 0, n_pieces = 0;
+  TriChunk *chunks = nullptr;     // plan construction only
+  int2 *pieces = nullptr;         // (triangles, k2 local index of the run's r2 mode)
+  TriDesc *descs = nullptr;       // [n_chunks], read by the kernel
   int n_items = 0;
-  TriItem *items = nullptr;       // [n_items], largest work first
+  TriItem *items = nullptr;       // [n_items]: grouped by tile count, largest work first in a group
+  int class_first[TRI_WARPS + 2] = {};  // items with n tiles: [class_first[n], class_first[n+1])
+  int class_stage[TRI_WARPS + 1] = {};  // stage size (complex values) of the CTAs with n tiles
   long long n_part = 0;
   double *part = nullptr;         // [n_part] partial sums
-  int max_row = 0;                // max L1+L2+L3 over items
-  int chunk = TRI_CHUNK;          // in-plane triangles per stage (fits shared memory)
   // per-realization buffers
   double *staging = nullptr;      // [n_modes][Q] complex128 rows of the r2c buffer
   double *S64 = nullptr;          // [n_modes][W] complex128 signed-plane mode data
@@ -104,6 +150,9 @@ struct beam_gpu_ctx {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
   size_t smem_optin = 0;
+  // side streams forked from `stream` for the per-class triangle-sum launches
+  cudaStream_t side[beam::TRI_WARPS] = {};
+  cudaEvent_t fork = nullptr, join[beam::TRI_WARPS] = {};
 };
 
 struct beam_gpu_plan {

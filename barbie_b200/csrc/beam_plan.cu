@@ -65,11 +65,32 @@ __global__ void k_tri_write(const TripletRef *trip, const int16_t *__restrict__ 
   }
 }
 
+// One copy descriptor per chunk from the chunk table, the triangle list and
+// the piece table.
+__global__ void k_build_desc(const TriChunk *__restrict__ chunks, long long n, const ushort4 *__restrict__ list,
+                             const int2 *__restrict__ pieces, TriDesc *__restrict__ out) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const TriChunk k = chunks[c];
+  const int nt = chunk_nt(k.packed), npc = chunk_npc(k.packed);
+  TriDesc d;
+  for (int j = 0; j < TRI_CHUNK; ++j) {
+    ushort4 e = j < nt ? list[k.t0 + j] : make_ushort4(0, 0, 0, 0);
+    d.xz[j][0] = e.x;
+    d.xz[j][1] = e.z;
+  }
+  for (int j = 0; j < TRI_PIECES; ++j) d.y[j] = j < npc ? (uint16_t)pieces[k.pc0 + j].y : (uint16_t)0;
+  d.packed = k.packed;
+  d.pad = 0;
+  out[c] = d;
+}
+
 // Count (and optionally list) the in-plane triangles of the given triplets.
 // mode tables (ring_first, mode_ij) must cover every ring the triplets use.
 static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, const std::vector<int32_t> &ring_first,
                               const int16_t *d_mode_ij, const int16_t *d_ringmap, const int16_t *d_pixlocal,
-                              std::vector<long long> &tri_first, ushort4 **d_list, long long *n_terms) {
+                              std::vector<long long> &tri_first, ushort4 **d_list, long long *n_terms,
+                              std::vector<int> *k2cnt) {
   cudaStream_t s = p->ctx->stream;
   const beam_geom &g = p->geom;
   std::vector<TripletRef> refs(rps.size());
@@ -119,6 +140,7 @@ static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, con
   }
   tri_first[refs.size()] = run;
   if (n_terms) *n_terms = run;
+  if (k2cnt) *k2cnt = cnt;
   if (d_list) {
     rc = dev_alloc(p, d_list, (size_t)run);
     if (rc == BEAM_OK) {
@@ -172,6 +194,247 @@ static int upload(beam_gpu_plan *p, T **dst, const std::vector<T> &src) {
   return BEAM_OK;
 }
 
+// Tiles, pieces, chunks and CTA work items of the triangle-sum kernel.
+//  * tiles: per ring triplet, its combos (p1, p2) placed on a grid of
+//    TRI_P1 planes p1 x 32 planes p3 (p3 = -p1-p2); tiles are grouped four p1
+//    blocks by two p3 windows per CTA so the staged row segments stay short;
+//  * runs: consecutive list entries sharing k2 (k2cnt, list order); a
+//    triplet's runs are split into `ns` contiguous ranges of about equal size
+//    when its work is large, so its CTAs share the triangle list;
+//  * pieces: runs cut to at most TRI_CHUNK triangles; chunks: whole pieces
+//    packed up to TRI_CHUNK triangles.
+// A = 16-byte unit of complex values (1 or 2); u_part receives the first
+// partial-sum slot of each triplet (ns_u * ncombo_u slots each).
+static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, const std::vector<int32_t> &u_ncombo,
+                      const std::vector<int32_t> &combo_p1, const std::vector<int32_t> &combo_p2,
+                      const std::vector<int> &k2cnt, int A, std::vector<int32_t> &u_nsplit,
+                      std::vector<long long> &u_part) {
+  const beam_geom &g = p->geom;
+  DevPlan &d = p->d;
+  auto floorA = [A](int v) { return v - (((v % A) + A) % A); };
+  auto ceilA = [&](int v) { return floorA(v + A - 1); };
+  struct Slot {
+    long long gkey, tkey;
+    int a, lane, c;
+  };
+  struct Group {
+    int tile0, ntiles;
+    int p1lo, p1hi, p3lo, p3hi, p2lo, p2hi;  // over accepted combos
+    int tp1lo, tp1hi;                        // first plane p1 of the tiles
+  };
+  std::vector<TriTile> tiles;
+  std::vector<int32_t> tile_combo;
+  std::vector<std::vector<Group>> groups(d.n_used);
+  std::vector<long long> k2base(d.n_used + 1, 0);
+  for (int u = 0; u < d.n_used; ++u) {
+    int r2 = g.rp[3 * p->used_rp[u] + 1];
+    k2base[u + 1] = k2base[u] + (p->ring_first[r2 + 1] - p->ring_first[r2]);
+  }
+  // tiles and groups
+  for (int u = 0; u < d.n_used; ++u) {
+    int cf = u_cfirst[u], nc = u_ncombo[u];
+    int p3min = 1 << 30;
+    for (int c = cf; c < cf + nc; ++c) p3min = std::min(p3min, -combo_p1[c] - combo_p2[c]);
+    std::vector<Slot> slots(nc);
+    for (int k = 0; k < nc; ++k) {
+      int c = cf + k, p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
+      long long bp1 = p1 / TRI_P1, bp3 = (p3 - p3min) / 32;
+      // a group is one window of 32 planes p3 over up to TRI_WARPS blocks of planes p1
+      slots[k] = Slot{bp3 * 1000000 + bp1 / TRI_WARPS, bp1 * 1000000 + bp3, p1 % TRI_P1, (p3 - p3min) % 32, c};
+    }
+    std::sort(slots.begin(), slots.end(), [](const Slot &x, const Slot &y) {
+      return x.gkey != y.gkey ? x.gkey < y.gkey : (x.tkey != y.tkey ? x.tkey < y.tkey : x.c < y.c);
+    });
+    for (size_t k = 0; k < slots.size();) {
+      Group gr{(int)tiles.size(), 0, 1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30),
+               1 << 30, -(1 << 30)};
+      long long gk = slots[k].gkey;
+      while (k < slots.size() && slots[k].gkey == gk) {
+        long long tk = slots[k].tkey;
+        int bp1 = (int)(tk / 1000000), bp3 = (int)(tk % 1000000);
+        tiles.push_back(TriTile{bp1 * TRI_P1, p3min + bp3 * 32});
+        tile_combo.resize(tiles.size() * TRI_P1 * 32, -1);
+        int32_t *tc = tile_combo.data() + (tiles.size() - 1) * TRI_P1 * 32;
+        for (; k < slots.size() && slots[k].tkey == tk && slots[k].gkey == gk; ++k) {
+          const Slot &s = slots[k];
+          tc[s.a * 32 + s.lane] = s.c;
+          int p1 = combo_p1[s.c], p2 = combo_p2[s.c], p3 = -p1 - p2;
+          gr.p1lo = std::min(gr.p1lo, p1); gr.p1hi = std::max(gr.p1hi, p1);
+          gr.p2lo = std::min(gr.p2lo, p2); gr.p2hi = std::max(gr.p2hi, p2);
+          gr.p3lo = std::min(gr.p3lo, p3); gr.p3hi = std::max(gr.p3hi, p3);
+        }
+        gr.tp1lo = std::min(gr.tp1lo, bp1 * TRI_P1);
+        gr.tp1hi = std::max(gr.tp1hi, bp1 * TRI_P1);
+        gr.ntiles++;
+      }
+      if (gr.ntiles > TRI_WARPS) {
+        set_detail("tile group larger than a CTA");
+        return BEAM_EINVAL;
+      }
+      groups[u].push_back(gr);
+    }
+  }
+  // splits, pieces, chunks, items
+  double total = 0.0;
+  for (int u = 0; u < d.n_used; ++u)
+    for (const Group &gr : groups[u]) total += (double)gr.ntiles * 256.0 * (double)(p->tri_first[u + 1] - p->tri_first[u]);
+  const double target = std::max(1.0, total / (std::max(1, p->ctx->num_sms) * 8.0));
+  std::vector<TriChunk> chunks;
+  std::vector<int2> pieces;
+  std::vector<TriItem> items;
+  std::vector<double> work;
+  u_nsplit.assign(d.n_used, 1);
+  u_part.assign(d.n_used + 1, 0);
+  for (int u = 0; u < d.n_used; ++u) {
+    const long long nt = p->tri_first[u + 1] - p->tri_first[u];
+    std::vector<int2> runs;  // (length, k2)
+    for (long long k = k2base[u]; k < k2base[u + 1]; ++k)
+      if (k2cnt[k] > 0) runs.push_back(make_int2(k2cnt[k], (int)(k - k2base[u])));
+    double wmax = 0.0;
+    for (const Group &gr : groups[u]) wmax = std::max(wmax, (double)gr.ntiles * 256.0 * (double)nt);
+    // split by work (load balance) and by list length (no CTA walks more than
+    // about TRI_TAU_MAX triangles: a CTA's time grows with its list, not its tiles)
+    double want = std::max(std::ceil(wmax / target), std::ceil((double)nt / TRI_TAU_MAX));
+    int ns = (int)std::min<double>(std::max(1.0, want), std::max<size_t>(1, runs.size()));
+    u_nsplit[u] = ns;
+    u_part[u + 1] = u_part[u] + (long long)ns * u_ncombo[u];
+    int rp = p->used_rp[u];
+    int m1 = p->ring_first[g.rp[3 * rp]], m2 = p->ring_first[g.rp[3 * rp + 1]], m3 = p->ring_first[g.rp[3 * rp + 2]];
+    size_t r = 0;
+    long long t = p->tri_first[u], done = 0;
+    for (int s = 0; s < ns; ++s) {
+      long long goal = nt * (s + 1) / ns;
+      int ch0 = (int)chunks.size();
+      // chunk under construction: triangles, pieces and piece lengths
+      long long ct0 = t;
+      int cpc0 = (int)pieces.size(), cnt_ = 0, cnpc = 0, clens = 0;
+      long long tsplit = 0;
+      auto close_chunk = [&]() {
+        chunks.push_back(TriChunk{ct0, cpc0, chunk_pack(cnt_, cnpc, clens)});
+        tsplit += cnt_;
+      };
+      while (r < runs.size() && (done < goal || s == ns - 1)) {
+        int left = runs[r].x;
+        while (left > 0) {
+          int len = std::min(left, TRI_CHUNK);
+          if (cnt_ + len > TRI_CHUNK || cnpc == TRI_PIECES) {
+            close_chunk();
+            ct0 = t;
+            cpc0 = (int)pieces.size();
+            cnt_ = cnpc = clens = 0;
+          }
+          pieces.push_back(make_int2(len, runs[r].y));
+          clens |= len << (5 * cnpc);
+          cnt_ += len;
+          cnpc += 1;
+          t += len;
+          left -= len;
+        }
+        done += runs[r].x;
+        ++r;
+      }
+      if (cnt_ > 0) close_chunk();
+      int ch1 = (int)chunks.size();
+      for (const Group &gr : groups[u]) {
+        TriItem it;
+        it.u = u;
+        it.split = s;
+        it.ch0 = ch0;
+        it.ch1 = ch1;
+        it.tile0 = gr.tile0;
+        it.ntiles = gr.ntiles;
+        it.m1 = m1;
+        it.m2 = m2;
+        it.m3 = m3;
+        // staged columns: x over the tiles' full p1 blocks (read warp-wide),
+        // z over the accepted p3, y over the accepted p2 widened by TRI_P1 - 1
+        // (a lane reads y for all TRI_P1 planes p1 of its tile)
+        const int cb = d.colbase, ext = TRI_P1 - 1;
+        it.colx = floorA(gr.tp1lo + cb); it.Lx = ceilA(gr.tp1hi + ext + cb + 1) - it.colx;
+        it.colz = floorA(gr.p3lo + cb); it.Lz = ceilA(gr.p3hi + cb + 1) - it.colz;
+        it.coly = floorA(gr.p2lo - ext + cb); it.Ly = ceilA(gr.p2hi + ext + cb + 1) - it.coly;
+        if (it.colx < 0 || it.colx + it.Lx > d.W || it.colz < 0 || it.colz + it.Lz > d.W || it.coly < 0 ||
+            it.coly + it.Ly > d.W)
+          return set_detail("staged columns outside the mode rows"), BEAM_EINVAL;
+        items.push_back(it);
+        work.push_back((double)gr.ntiles * 256.0 * (double)tsplit);
+      }
+    }
+  }
+  // consistency: every combo in exactly one tile slot, every triangle in exactly one chunk
+  {
+    std::vector<char> seen(combo_p1.size(), 0);
+    for (int32_t c : tile_combo)
+      if (c >= 0) {
+        if (seen[c]) return set_detail("combo placed twice"), BEAM_EINVAL;
+        seen[c] = 1;
+      }
+    for (char v : seen)
+      if (!v) return set_detail("combo without a tile"), BEAM_EINVAL;
+    long long covered = 0, piece_sum = 0;
+    for (const TriChunk &k : chunks) {
+      int nt = chunk_nt(k.packed), npc = chunk_npc(k.packed), lsum = 0;
+      covered += nt;
+      for (int j = 0; j < npc; ++j) {
+        piece_sum += pieces[k.pc0 + j].x;
+        lsum += chunk_len(k.packed, j);
+        if (chunk_len(k.packed, j) != pieces[k.pc0 + j].x) return set_detail("packed piece length"), BEAM_EINVAL;
+      }
+      if (lsum != nt) return set_detail("chunk length"), BEAM_EINVAL;
+    }
+    if (covered != d.n_terms || piece_sum != d.n_terms) return set_detail("chunks do not cover the triangle lists"), BEAM_EINVAL;
+  }
+  // grouped by tile count (one launch per count, CTAs of that many warps),
+  // largest work first within a group so each launch ends on small items
+  std::vector<int> order(items.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return items[a].ntiles != items[b].ntiles ? items[a].ntiles < items[b].ntiles : work[a] > work[b];
+  });
+  std::vector<TriItem> sorted(items.size());
+  for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
+  size_t elem = (A == 2) ? 8 : 16;
+  size_t budget = p->ctx->smem_optin > 4096 ? p->ctx->smem_optin - 4096 : 48 * 1024;
+  for (int n = 0; n <= TRI_WARPS + 1; ++n) d.class_first[n] = 0;
+  for (int n = 0; n <= TRI_WARPS; ++n) d.class_stage[n] = 0;
+  for (const TriItem &it : sorted) {
+    d.class_first[it.ntiles + 1]++;
+    int stage = TRI_CHUNK * (it.Lx + it.Lz) + TRI_PIECES * it.Ly;
+    d.class_stage[it.ntiles] = std::max(d.class_stage[it.ntiles], stage);
+  }
+  for (int n = 0; n <= TRI_WARPS; ++n) d.class_first[n + 1] += d.class_first[n];
+  for (int n = 1; n <= TRI_WARPS; ++n)
+    if ((size_t)TRI_STAGES * d.class_stage[n] * elem + sizeof(double) * TRI_P1 * 32 * n > budget) {
+      set_detail("staged mode rows do not fit shared memory");
+      return BEAM_EINVAL;
+    }
+  d.n_tiles = (int)tiles.size();
+  d.n_chunks = (long long)chunks.size();
+  d.n_pieces = (long long)pieces.size();
+  d.n_items = (int)sorted.size();
+  BEAM_TRY(upload(p, &d.tiles, tiles));
+  BEAM_TRY(upload(p, &d.tile_combo, tile_combo));
+  BEAM_TRY(upload(p, &d.chunks, chunks));
+  BEAM_TRY(upload(p, &d.pieces, pieces));
+  BEAM_TRY(upload(p, &d.items, sorted));
+  // per-chunk copy descriptors; the list, chunk and piece tables are then no longer needed
+  BEAM_TRY(dev_alloc(p, &d.descs, (size_t)d.n_chunks));
+  if (d.n_chunks) {
+    k_build_desc<<<(unsigned)((d.n_chunks + 255) / 256), 256, 0, p->ctx->stream>>>(d.chunks, d.n_chunks, d.tri_list,
+                                                                                   d.pieces, d.descs);
+    BEAM_CUDA(cudaGetLastError());
+    BEAM_CUDA(cudaStreamSynchronize(p->ctx->stream));
+  }
+  cudaFree(d.chunks);
+  cudaFree(d.pieces);
+  cudaFree(d.tri_list);
+  p->device_bytes -= sizeof(TriChunk) * d.n_chunks + sizeof(int2) * d.n_pieces + sizeof(ushort4) * d.n_terms;
+  d.chunks = nullptr;
+  d.pieces = nullptr;
+  d.tri_list = nullptr;
+  return BEAM_OK;
+}
+
 int build_plan_tables(beam_gpu_plan *p) {
   const beam_geom &g = p->geom;
   DevPlan &d = p->d;
@@ -195,7 +458,8 @@ int build_plan_tables(beam_gpu_plan *p) {
   auto floorA = [A](int v) { return v - (((v % A) + A) % A); };
   auto ceilA = [A, &floorA](int v) { return floorA(v + A - 1); };
   d.Q = Q;
-  d.W = ceilA(2 * Q - 1);
+  d.colbase = Q - 1 + TRI_PAD;
+  d.W = ceilA(2 * Q - 1 + 2 * TRI_PAD);
 
   std::vector<int16_t> pixlocal;
   build_modes(g, ring_on, p->ring_first, p->mode_ij, pixlocal);
@@ -262,9 +526,10 @@ int build_plan_tables(beam_gpu_plan *p) {
   std::vector<int32_t> combo_out(ntri);
   for (long long c = 0; c < ntri; ++c) combo_out[c] = p->bin_pos[combo_tid[c]];
 
-  // in-plane triangle lists (GPU)
+  // in-plane triangle lists (GPU), k2-major: k2cnt holds each run's length
+  std::vector<int> k2cnt;
   BEAM_TRY(enumerate_in_plane(p, p->used_rp, p->ring_first, d.mode_ij, d.ringmap, d.pixlocal, p->tri_first,
-                              &d.tri_list, &d.n_terms));
+                              &d.tri_list, &d.n_terms, &k2cnt));
 
   // epilogue tables in bin order
   std::vector<double> ep_px(ntri), ep_pz(ntri);
@@ -277,84 +542,14 @@ int build_plan_tables(beam_gpu_plan *p) {
     ep_cnt[i] = (int32_t)(p->tri_first[u + 1] - p->tri_first[u]);
   }
 
-  // work items: split large (triplet) work along its triangle list
-  int n_sms = std::max(1, p->ctx->num_sms);
-  long double total = 0;
-  for (int u = 0; u < d.n_used; ++u)
-    total += (long double)u_ncombo[u] * (long double)(p->tri_first[u + 1] - p->tri_first[u]);
-  long double target = std::max<long double>(total / (n_sms * 6.0L), 1.0L);
-  std::vector<TriItem> items;
-  std::vector<int32_t> u_nsplit(d.n_used, 1);
-  std::vector<long long> u_part(d.n_used + 1, 0);
-  std::vector<long double> item_work;
-  const int max_combos = TRI_THREADS * TRI_MAX_SLOTS;
-  int max_row = 1;
-  for (int u = 0; u < d.n_used; ++u) {
-    long long nt = p->tri_first[u + 1] - p->tri_first[u];
-    long double w = (long double)u_ncombo[u] * (long double)nt;
-    int ncg = (u_ncombo[u] + max_combos - 1) / max_combos;  // combo groups
-    long long ns = (long long)std::ceil((double)(w / (target * ncg)));
-    ns = std::max<long long>(1, std::min<long long>(ns, std::max<long long>(1, nt / (4 * TRI_CHUNK))));
-    u_nsplit[u] = (int)ns;
-    u_part[u + 1] = u_part[u] + ns * (long long)u_ncombo[u];
-    int rp = p->used_rp[u];
-    int r1 = g.rp[3 * rp], r2 = g.rp[3 * rp + 1], r3 = g.rp[3 * rp + 2];
-    for (int cg = 0; cg < ncg; ++cg) {
-      int c0 = u_cfirst[u] + cg * max_combos, c1 = std::min(u_cfirst[u + 1], c0 + max_combos);
-      int p1lo = 1 << 30, p1hi = -(1 << 30), p2lo = 1 << 30, p2hi = -(1 << 30), p3lo = 1 << 30, p3hi = -(1 << 30);
-      for (int c = c0; c < c1; ++c) {
-        int a = combo_p1[c], b = combo_p2[c], e = -a - b;
-        p1lo = std::min(p1lo, a); p1hi = std::max(p1hi, a);
-        p2lo = std::min(p2lo, b); p2hi = std::max(p2hi, b);
-        p3lo = std::min(p3lo, e); p3hi = std::max(p3hi, e);
-      }
-      for (long long s = 0; s < ns; ++s) {
-        TriItem it;
-        it.u = u;
-        it.split = (int)s;
-        it.c0 = c0;
-        it.c1 = c1;
-        it.t0 = p->tri_first[u] + nt * s / ns;
-        it.t1 = p->tri_first[u] + nt * (s + 1) / ns;
-        it.m1 = p->ring_first[r1];
-        it.m2 = p->ring_first[r2];
-        it.m3 = p->ring_first[r3];
-        // column ranges of the signed-plane rows (column of plane q is q + Q - 1)
-        it.p1lo = floorA(p1lo + Q - 1); it.L1 = ceilA(p1hi + Q) - it.p1lo;
-        it.p2lo = floorA(p2lo + Q - 1); it.L2 = ceilA(p2hi + Q) - it.p2lo;
-        it.p3lo = floorA(p3lo + Q - 1); it.L3 = ceilA(p3hi + Q) - it.p3lo;
-        max_row = std::max(max_row, it.L1 + it.L2 + it.L3);
-        items.push_back(it);
-        item_work.push_back((long double)(c1 - c0) * (long double)(it.t1 - it.t0));
-      }
-    }
-  }
-  // largest first, so the tail of the launch holds the small items
-  std::vector<int> order(items.size());
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return item_work[a] > item_work[b]; });
-  std::vector<TriItem> sorted(items.size());
-  for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
-  d.n_items = (int)sorted.size();
-  d.max_row = max_row;
-  {
-    // two pipeline stages of `chunk` triangle rows must fit the opt-in shared memory
-    size_t elem = (A == 2) ? 8 : 16;
-    size_t budget = p->ctx->smem_optin > 4096 ? p->ctx->smem_optin - 4096 : 48 * 1024;
-    size_t fit = budget / (2 * (size_t)max_row * elem);
-    if (fit < 1) {
-      set_detail("signed-plane rows too long for shared memory");
-      return BEAM_EINVAL;
-    }
-    d.chunk = (int)std::min<size_t>(TRI_CHUNK, fit);
-  }
+  // work decomposition of the triangle-sum kernel
+  std::vector<int32_t> u_nsplit;
+  std::vector<long long> u_part;
+  BEAM_TRY(build_work(p, u_cfirst, u_ncombo, combo_p1, combo_p2, k2cnt, A, u_nsplit, u_part));
   d.n_part = u_part[d.n_used];
   u_part.pop_back();
   u_cfirst.pop_back();
 
-  BEAM_TRY(upload(p, &d.items, sorted));
-  BEAM_TRY(upload(p, &d.combo_p1, combo_p1));
-  BEAM_TRY(upload(p, &d.combo_p2, combo_p2));
   BEAM_TRY(upload(p, &d.combo_u, combo_u));
   BEAM_TRY(upload(p, &d.combo_out, combo_out));
   BEAM_TRY(upload(p, &d.u_cfirst, u_cfirst));
@@ -386,9 +581,10 @@ int build_plan_tables(beam_gpu_plan *p) {
 
 void free_plan_tables(beam_gpu_plan *p) {
   DevPlan &d = p->d;
-  void *ptrs[] = {d.mode_ij, d.mode_neg, d.ringmap, d.pixlocal, d.tri_list, d.combo_p1, d.combo_p2, d.combo_u,
-                  d.combo_out, d.u_cfirst, d.u_ncombo, d.u_nsplit, d.u_part, d.items, d.part, d.staging, d.S64,
-                  d.S32, d.B, d.bin_first, d.ep_px, d.ep_pz, d.ep_cnt, d.bins, d.bin_count, d.status};
+  void *ptrs[] = {d.mode_ij, d.mode_neg, d.ringmap, d.pixlocal, d.tri_list, d.combo_u, d.combo_out, d.u_cfirst,
+                  d.u_ncombo, d.u_nsplit, d.u_part, d.tiles, d.tile_combo, d.chunks, d.pieces, d.descs, d.items, d.part,
+                  d.staging, d.S64, d.S32, d.B, d.bin_first, d.ep_px, d.ep_pz, d.ep_cnt, d.bins, d.bin_count,
+                  d.status};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (p->h_staging) cudaFreeHost(p->h_staging);
@@ -414,7 +610,7 @@ int count_closed_triangles(beam_gpu_plan *p, std::vector<long long> &counts) {
   std::iota(rps.begin(), rps.end(), 0);
   std::vector<long long> first;
   size_t before = p->device_bytes;
-  int rc = enumerate_in_plane(p, rps, ring_first, d_mode, p->d.ringmap, nullptr, first, nullptr, nullptr);
+  int rc = enumerate_in_plane(p, rps, ring_first, d_mode, p->d.ringmap, nullptr, first, nullptr, nullptr, nullptr);
   p->device_bytes = before;
   cudaFree(d_mode);
   if (rc != BEAM_OK) return rc;

@@ -1,0 +1,289 @@
+// Triangle-sum kernel of libbeam_gpu (sm_100a): for every accepted triangle of
+// the reference loop, the in-plane closed-triangle sum
+//   B = NN^2 Re sum_{k1+k2+k3=0} x_{k1}(p1) y_{k2}(p2) z_{k3}(p3)
+// which equals the pixel sum of barbie.c:329-337 (see beam_plan.cu).
+//
+// A CTA takes one work item: n tiles of one ring triplet (r1, r2, r3) over a
+// range of its in-plane triangle list, with n consumer warps (one per tile)
+// and one producer warp. The list is k2-major, cut into pieces (runs of one
+// k2) and chunks (<= TRI_CHUNK triangles, <= TRI_PIECES pieces) described by
+// TriDesc records. The producer streams chunks into a TRI_STAGES-deep ring of
+// shared stages with TMA bulk copies -- per triangle the r1 row of k1 over the
+// CTA's planes p1 and the r3 row of k3 over its planes p3, per piece the r2 row
+// of k2 over its planes p2 -- completing on full[s] (transaction bytes). Each
+// consumer releases a stage on empty[s]; the producer refills it when all have.
+//
+// A consumer thread owns the combos (p1_0 + q, p3_0 + lane), q < TRI_P1, of
+// its tile. Over a piece it accumulates w[q] += x_{k1}(p1_0+q) * z_{k3}(p3)
+// (4 FMA; x read warp-wide from one address) and at the end of the piece adds
+// Re(y_{k2}(-p1_0-q-p3) * w[q]) to its sums.
+#include "beam_device.cuh"
+#include "beam_internal.h"
+
+namespace beam {
+
+template <typename C>
+struct TriAcc;
+template <>
+struct TriAcc<double2> {
+  typedef double t;
+};
+template <>
+struct TriAcc<float2> {
+  typedef float t;
+};
+
+struct TriArgs {
+  const TriItem *items;  // this launch's items
+  const TriTile *tiles;
+  const int32_t *tile_combo;
+  const TriDesc *descs;
+  const void *S;
+  int W;
+  int colbase;  // column of plane 0 in a signed-plane row
+  const int32_t *u_cfirst, *u_ncombo;
+  const long long *u_part;
+  double *part;
+  int *status;
+  int stage;  // complex values per stage
+};
+
+// What the producer needs to issue one chunk's copies, loaded one chunk ahead
+// of the issue with independent loads: the chunk layout, and for this lane the
+// mode rows of triangle `lane` (x: ring r1, z: ring r3) and of piece `lane` (y).
+struct TriMeta {
+  int packed;
+  uint32_t xz;  // k1 | k3 << 16
+  int y;
+};
+
+__device__ __forceinline__ TriMeta tri_meta(const TriArgs &a, int ch) {
+  const int lane = threadIdx.x & 31;
+  const TriDesc *d = a.descs + ch;
+  TriMeta m;
+  m.packed = d->packed;
+  m.xz = lane < TRI_CHUNK ? *reinterpret_cast<const uint32_t *>(&d->xz[lane][0]) : 0u;
+  m.y = lane < TRI_PIECES ? d->y[lane] : 0;
+  return m;
+}
+
+template <typename C>
+__device__ __forceinline__ void tri_issue(const TriArgs &a, const TriItem &it, const C *S, C *st, uint32_t full,
+                                          const TriMeta &m) {
+  const int lane = threadIdx.x & 31;
+  const int nt = chunk_nt(m.packed), npc = chunk_npc(m.packed);
+  C *xs = st, *zs = st + TRI_CHUNK * it.Lx, *ys = zs + TRI_CHUNK * it.Lz;
+  if (lane == 0) mbar_expect_tx(full, (uint32_t)((nt * (it.Lx + it.Lz) + npc * it.Ly) * sizeof(C)));
+  __syncwarp();
+  if (lane < nt) {
+    const int mx = it.m1 + (int)(m.xz & 0xffffu), mz = it.m3 + (int)(m.xz >> 16);
+    bulk_g2s(smem_addr(xs + lane * it.Lx), S + (size_t)mx * a.W + it.colx, (uint32_t)(it.Lx * sizeof(C)), full);
+    bulk_g2s(smem_addr(zs + lane * it.Lz), S + (size_t)mz * a.W + it.colz, (uint32_t)(it.Lz * sizeof(C)), full);
+  }
+  if (lane < npc)
+    bulk_g2s(smem_addr(ys + lane * it.Ly), S + (size_t)(it.m2 + m.y) * a.W + it.coly, (uint32_t)(it.Ly * sizeof(C)),
+             full);
+}
+
+template <typename C>
+__global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a) {
+  typedef typename TriAcc<C>::t acc_t;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t full[TRI_STAGES], empty[TRI_STAGES];
+  __shared__ volatile int s_fail;
+  const TriItem it = a.items[blockIdx.x];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ncons = (blockDim.x >> 5) - 1;  // consumer warps == it.ntiles; warp ncons produces
+  if (tid == 0) {
+    for (int s = 0; s < TRI_STAGES; ++s) {
+      mbar_init(smem_addr(&full[s]), 1);
+      mbar_init(smem_addr(&empty[s]), ncons);
+    }
+    s_fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  C *stages = reinterpret_cast<C *>(smem_raw);
+  const C *S = static_cast<const C *>(a.S);
+  const int nch = it.ch1 - it.ch0;
+
+  if (warp == ncons) {
+    // ------------------------------------------------------------ producer
+    int issued = 0;
+    bool failed = false;
+    TriMeta meta = nch > 0 ? tri_meta(a, it.ch0) : TriMeta{0, 0u, 0};
+    for (int c = 0; c < nch; ++c) {
+      const int s = c % TRI_STAGES;
+      if (c >= TRI_STAGES &&
+          (s_fail || !mbar_wait_bounded(smem_addr(&empty[s]), (uint32_t)(((c / TRI_STAGES) - 1) & 1)))) {
+        failed = true;
+        break;
+      }
+      const TriMeta cur = meta;
+      if (c + 1 < nch) meta = tri_meta(a, it.ch0 + c + 1);
+      tri_issue<C>(a, it, S, stages + s * a.stage, smem_addr(&full[s]), cur);
+      issued = c + 1;
+    }
+    if (failed) {
+      s_fail = 1;
+      if (lane == 0) atomicOr(a.status, DEV_TIMEOUT);
+      // let the copies in flight (the last TRI_STAGES issued) land before the
+      // CTA's shared memory can be released
+      for (int c = issued - TRI_STAGES > 0 ? issued - TRI_STAGES : 0; c < issued; ++c)
+        mbar_wait_bounded(smem_addr(&full[c % TRI_STAGES]), (uint32_t)((c / TRI_STAGES) & 1));
+    }
+    return;
+  }
+
+  // -------------------------------------------------------------- consumer
+  // columns of this thread's reads in the staged rows
+  const TriTile tl = a.tiles[it.tile0 + warp];
+  const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + lane;
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < TRI_P1; ++q) any |= (tc[q * 32] >= 0);
+  const int p3 = tl.p3_0 + lane;
+  const int ox0 = tl.p1_0 + a.colbase - it.colx;                          // x reads ox0 + q
+  const int oz = any ? p3 + a.colbase - it.colz : 0;                      // z read
+  const int oy0 = any ? -tl.p1_0 - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
+  // per-thread sums in shared memory ([q][thread]): they change once per piece
+  double *sum = reinterpret_cast<double *>(smem_raw + (size_t)TRI_STAGES * a.stage * sizeof(C)) + tid;
+  const int sstride = 32 * ncons;
+#pragma unroll
+  for (int q = 0; q < TRI_P1; ++q) sum[q * sstride] = 0.0;
+
+  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
+  for (int c = 0; c < nch; ++c) {
+    const int s = c % TRI_STAGES;
+    const int packed = packed_next;  // piece layout of this chunk, loaded one chunk ahead
+    if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
+    if (s_fail || !mbar_wait_bounded(smem_addr(&full[s]), (uint32_t)((c / TRI_STAGES) & 1))) {
+      s_fail = 1;
+      if (lane == 0) atomicOr(a.status, DEV_TIMEOUT);
+      return;
+    }
+    const C *xs = stages + s * a.stage;
+    const C *zs = xs + TRI_CHUNK * it.Lx;
+    const C *ys = zs + TRI_CHUNK * it.Lz;
+    const int npc = chunk_npc(packed);
+    int tt = 0;
+    for (int pc = 0; pc < npc; ++pc) {
+      const int len = chunk_len(packed, pc);
+      acc_t wr[TRI_P1], wi[TRI_P1];
+#pragma unroll
+      for (int q = 0; q < TRI_P1; ++q) wr[q] = wi[q] = (acc_t)0;
+      for (int j = 0; j < len; ++j, ++tt) {
+        const C z = zs[tt * it.Lz + oz];
+        const C *xr = xs + tt * it.Lx + ox0;
+#pragma unroll
+        for (int q = 0; q < TRI_P1; ++q) {
+          const C x = xr[q];
+          wr[q] = fma(x.x, z.x, fma(-x.y, z.y, wr[q]));
+          wi[q] = fma(x.x, z.y, fma(x.y, z.x, wi[q]));
+        }
+      }
+      const C *yr = ys + pc * it.Ly + oy0;
+#pragma unroll
+      for (int q = 0; q < TRI_P1; ++q) {
+        const C y = yr[-q];
+        sum[q * sstride] += (double)fma(y.x, wr[q], -y.y * wi[q]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
+  }
+  const int nc = a.u_ncombo[it.u];
+  double *out = a.part + a.u_part[it.u] + (long long)it.split * nc - a.u_cfirst[it.u];
+#pragma unroll
+  for (int q = 0; q < TRI_P1; ++q) {
+    const int cidx = tc[q * 32];
+    if (cidx >= 0) out[cidx] = sum[q * sstride];
+  }
+}
+
+// Sum the splits of each combo in split order, scale by NN^2 and store the
+// triangle's B at its bin-order position.
+__global__ void k_reduce(long long n_combo, const int32_t *__restrict__ combo_u, const int32_t *__restrict__ u_cfirst,
+                         const int32_t *__restrict__ u_ncombo, const int32_t *__restrict__ u_nsplit,
+                         const long long *__restrict__ u_part, const int32_t *__restrict__ combo_out,
+                         const double *__restrict__ part, double nn2, double *__restrict__ B) {
+  long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n_combo) return;
+  int u = combo_u[c];
+  int nc = u_ncombo[u], ns = u_nsplit[u];
+  const double *p = part + u_part[u] + (c - u_cfirst[u]);
+  double s = 0.0;
+  for (int k = 0; k < ns; ++k) s += p[(long long)k * nc];
+  B[combo_out[c]] = nn2 * s;
+}
+
+template <typename C>
+static size_t tri_smem(int stage, int ntiles) {
+  return (size_t)TRI_STAGES * stage * sizeof(C) + sizeof(double) * TRI_P1 * 32 * ntiles;
+}
+
+// One launch per tile count n (CTAs of n consumer warps + 1 producer warp), on
+// side streams forked from and joined back into the context's stream, so the
+// launches overlap.
+template <typename C>
+static int launch_classes(beam_gpu_plan *p, TriArgs a) {
+  DevPlan &d = p->d;
+  beam_gpu_ctx *ctx = p->ctx;
+  size_t max_smem = 0;
+  for (int n = 1; n <= TRI_WARPS; ++n) max_smem = std::max(max_smem, tri_smem<C>(d.class_stage[n], n));
+  BEAM_CUDA(cudaFuncSetAttribute(k_triangle<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+  BEAM_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
+  for (int n = TRI_WARPS; n >= 1; --n) {
+    int first = d.class_first[n], count = d.class_first[n + 1] - first;
+    if (count == 0) continue;
+    cudaStream_t st = ctx->side[n - 1];
+    BEAM_CUDA(cudaStreamWaitEvent(st, ctx->fork, 0));
+    TriArgs b = a;
+    b.items = d.items + first;
+    b.stage = d.class_stage[n];
+    k_triangle<C><<<count, 32 * (n + 1), tri_smem<C>(b.stage, n), st>>>(b);
+    BEAM_CUDA(cudaGetLastError());
+    BEAM_CUDA(cudaEventRecord(ctx->join[n - 1], st));
+    BEAM_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[n - 1], 0));
+  }
+  return BEAM_OK;
+}
+
+int run_triangle_sums(beam_gpu_plan *p) {
+  DevPlan &d = p->d;
+  cudaStream_t s = p->ctx->stream;
+  if (d.n_combo == 0) {
+    for (int k = 1; k <= 3; ++k) mark(p, k);
+    return BEAM_OK;
+  }
+  TriArgs a;
+  a.items = d.items;
+  a.tiles = d.tiles;
+  a.tile_combo = d.tile_combo;
+  a.descs = d.descs;
+  a.W = d.W;
+  a.colbase = d.colbase;
+  a.u_cfirst = d.u_cfirst;
+  a.u_ncombo = d.u_ncombo;
+  a.u_part = d.u_part;
+  a.part = d.part;
+  a.status = d.status;
+  a.stage = 0;
+  mark(p, 1);
+  if (d.S64) {
+    a.S = d.S64;
+    BEAM_TRY(launch_classes<double2>(p, a));
+  } else {
+    a.S = d.S32;
+    BEAM_TRY(launch_classes<float2>(p, a));
+  }
+  mark(p, 2);
+  double nn2 = (double)p->geom.NN * (double)p->geom.NN;
+  k_reduce<<<(unsigned)((d.n_combo + 255) / 256), 256, 0, s>>>(d.n_combo, d.combo_u, d.u_cfirst, d.u_ncombo,
+                                                               d.u_nsplit, d.u_part, d.combo_out, d.part, nn2, d.B);
+  BEAM_CUDA(cudaGetLastError());
+  mark(p, 3);
+  return BEAM_OK;
+}
+
+}  // namespace beam

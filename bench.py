@@ -1,0 +1,425 @@
+#!/usr/bin/env python3
+"""Throughput benchmark of the BEAM bispectrum estimator hot path on B200.
+
+Workload: one bispectrum = all 16 (l,m) multipoles over all (k1, t, mu) bins of
+one realization at NN=384, Nmax=100 planes, Nr=40 rings, k1 bins 1..51 of
+width 1, 5 t and mu bins: the reference example `barbie 384 1 51 1 1`.
+Inputs are seeded synthetic fields in the reference's r2c input layout (no
+public dataset is involved).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm prints one JSON line: `value` is bispectra/hour with the r2c buffers
+resident in HBM (the plain FP64 path, 1e-10 of the reference); `e2e` is the
+same through the C ABI from pinned host buffers (host gather + H2D + compute +
+D2H of the bins); `mixed` is the FP32 path with its error against FP64 per
+(l,m,bin); `roofline` is the triangle-sum kernel against the measured FP64
+peak; `cpu_baseline` is the oracle's CPU restatement timed on a bounded sample.
+Each rank processes its own realizations (weak scaling, no collective on the
+data path).
+
+The reference arm (--impl reference) times the reference program itself
+(oracle/_ref/barbie_ref, built from the reference's sources) on bounded
+samples of the same workload on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(NN=384, Nmax=100, Nr=40, UL_k1=51, LL_k1=1, BW_k1=1, n_mtbin=5)
+METRIC = "bispectra/hour @NN=384 (mixed vs FP64, 1 B200, rel err<=1e-5); p50/p99 latency"
+UNIT = "bispectra/hour"
+WORKLOAD_NAME = "barbie 384 1 51 1 1: NN=384, Nmax=100, Nr=40, k1 bins 1..51 width 1, 5 t x 5 mu bins, 16 (l,m)"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--fields", type=int, default=2, help="realizations per rank, cycled over the steps")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="beam_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].split()[0].isdigit():
+                    rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [int(r[1].split()[0]) for r in rows]
+        mx = [int(r[2].split()[0]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        power = [float(r[3].split()[0]) for r in rows if r[3].split()[0].replace(".", "").isdigit()]
+        return {"sm_mhz": int(statistics.median(sm)), "sm_max_mhz": max(mx), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(power) if power else None}
+
+
+# ------------------------------------------------------------------- helpers
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_fp64_peak(torch, device) -> float:
+    """cuBLAS DGEMM throughput (TFLOP/s), best of 5 at 8192^3."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per launch of a kernel from a committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_nn384.txt")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        for line in fh:
+            m = re.match(r"\s*dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", line)
+            if m:
+                return float(m.group(1))
+    return None
+
+
+def mixed_errors(fp64: dict, mixed: dict) -> dict:
+    """Relative error of the mixed path against FP64 per (l,m,bin), printed bins only."""
+    ok = (fp64["norm"][..., 0] > 0.1)[..., None] & np.isfinite(fp64["out"]) & (fp64["out"] != 0)
+    ok = np.broadcast_to(ok, fp64["out"].shape)
+    rel = np.full(fp64["out"].shape, np.nan)
+    rel[ok] = np.abs(mixed["out"][ok] - fp64["out"][ok]) / np.abs(fp64["out"][ok])
+    per_lm = [float(np.nanmax(rel[..., k])) if np.any(ok[..., k]) else None for k in range(16)]
+    r = rel[ok]
+    return {"max_rel_err": float(r.max()), "p99_rel_err": float(np.quantile(r, 0.99)),
+            "median_rel_err": float(np.median(r)), "frac_within_1e-5": float(np.mean(r <= 1e-5)),
+            "max_rel_err_per_lm": per_lm, "bins_compared": int(r.size),
+            "counts_identical": bool(np.array_equal(fp64["count"], mixed["count"]))}
+
+
+# --------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from barbie_b200 import beam
+    from barbie_b200.synth import realization_seed, synth_field
+
+    world, rank, local = dist_setup(args)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    W = WORKLOAD
+    ctx = beam.Context(local)
+    plan = beam.Plan(ctx, W["NN"], W["UL_k1"], W["LL_k1"], W["BW_k1"], Nmax=W["Nmax"], Nr=W["Nr"],
+                     n_mtbin=W["n_mtbin"])
+    info = plan.info
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    fields = [synth_field(W["NN"], realization_seed(1 + rank * args.fields + i)) for i in range(args.fields)]
+    dev_fields = [torch.from_numpy(f).to(dev) for f in fields]
+    host_fields = [torch.from_numpy(f).pin_memory() for f in fields]
+    host_np = [h.numpy() for h in host_fields]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+
+    def timed_loop(p, srcs, steps):
+        times, tri = [], []
+        for i in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p.run(srcs[i % len(srcs)])
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            tri.append(p.last_timings()["triangle"])
+        return times, tri
+
+    # warm-up, then the timed device-resident loop
+    timed_loop(plan, dev_fields, args.warmup)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    wall0 = time.perf_counter()
+    times, tri_ms = timed_loop(plan, dev_fields, args.steps)
+    barrier()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    total_ms = max_over_ranks(sum(times))
+    value = world * args.steps / (total_ms / 1e3) * 3600.0
+
+    # end to end through the C ABI from pinned host buffers
+    timed_loop(plan, host_np, 1)
+    barrier()
+    e2e_times, _ = timed_loop(plan, host_np, args.steps)
+    barrier()
+    e2e_total = max_over_ranks(sum(e2e_times))
+    e2e_value = world * args.steps / (e2e_total / 1e3) * 3600.0
+    h2d = info["n_modes"] * info["n_planes"] * 16
+    d2h = info["n_bins"] * (3 * 16 * 8 + 8)
+
+    # latency percentiles of single jobs (device-resident and e2e)
+    lat = {"p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
+           "e2e_p50_ms": float(np.percentile(e2e_times, 50)), "e2e_p99_ms": float(np.percentile(e2e_times, 99))}
+
+    # mixed precision path
+    mixed = None
+    if not args.no_mixed:
+        plan_m = beam.Plan(ctx, W["NN"], W["UL_k1"], W["LL_k1"], W["BW_k1"], Nmax=W["Nmax"], Nr=W["Nr"],
+                           n_mtbin=W["n_mtbin"], precision="mixed")
+        timed_loop(plan_m, dev_fields, args.warmup)
+        barrier()
+        mt, mtri = timed_loop(plan_m, dev_fields, args.steps)
+        barrier()
+        m_total = max_over_ranks(sum(mt))
+        ref = plan.run(dev_fields[0])
+        got = plan_m.run(dev_fields[0])
+        mixed = {"value": world * args.steps / (m_total / 1e3) * 3600.0, "unit": UNIT,
+                 "ms_per_step": m_total / args.steps, "triangle_kernel_ms": float(np.mean(mtri)),
+                 "speedup_vs_fp64": (sum(times) / sum(mt)), **mixed_errors(ref, got)}
+        plan_m.close()
+
+    # roofline of the dominant kernel (triangle sums, FP64 pipe)
+    peak = measured_fp64_peak(torch, dev)
+    tri_avg = float(np.mean(tri_ms))
+    flops = 10.0 * info["n_fourier_terms"]  # complex a*b (6) + Re(ab*c) (3) + accumulate (1)
+    achieved = flops / (tri_avg / 1e3) / 1e12
+    roofline = {"kernel": "k_triangle<double2>", "bound": "fp64", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": profile_traffic("k_triangle"),
+                "flops_per_launch": flops, "launch_ms": tri_avg,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "pixel_equivalent_tflops": 4.0 * info["n_triples"] * W["NN"] ** 2 / (tri_avg / 1e3) / 1e12}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(fields[0], info)
+
+    gpu_launches = 4 * args.steps  # build_modes, triangle, reduce, epilogue per step
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, **W, "path": "plain FP64, closed in-plane triangle sums",
+                   "parallelism": f"replicas x{world} (one realization per rank per step)",
+                   "l2": "flushed between steps (256 MiB write, outside the timed events)",
+                   "n_triples": info["n_triples"], "n_fourier_terms": info["n_fourier_terms"],
+                   "plan_device_bytes": info["device_bytes"]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_total / args.steps},
+        "latency": lat, "wall_s": wall, "clocks": clk, "roofline": roofline, "mixed": mixed,
+        "cpu_baseline": cpu, "gpu_launches": gpu_launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline_port(field, info):
+    """The oracle (CPU restatement of the reference) timed on a bounded random
+    sample of accepted triangles, transforms and pixel sums over all host cores,
+    extrapolated to one full bispectrum."""
+    from oracle import oracle_py
+    W = WORKLOAD
+    cores = os.cpu_count() or 1
+    ntri = info["n_triples"]
+    nsample = int(min(ntri, 1500 * cores))
+    rng = np.random.default_rng(2024)
+    sample = np.sort(rng.choice(ntri, size=nsample, replace=False))
+    r = oracle_py.time_sample(field, W["NN"], W["Nmax"], W["Nr"], W["UL_k1"], W["LL_k1"], W["BW_k1"], sample, cores)
+    n_arrays = W["Nmax"] * W["Nr"]  # wrapid_fast builds every (plane, ring) array
+    secs = ntri * r["t_sum"] / nsample + n_arrays * r["t_fft"] / max(1, r["n_fft"])
+    return {"value": 3600.0 / secs, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{nsample} random accepted triangles of {ntri} (pixel sums) and the {r['n_fft']} plane-ring "
+                      f"transforms they need, extrapolated to {ntri} triangles and {n_arrays} transforms",
+            "sample_seconds": r["t_sum"] + r["t_fft"], "seconds_per_bispectrum": secs}
+
+
+# --------------------------------------------------------------- reference
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return
+    from oracle import oracle_py
+    ref_bin = oracle_py.REF_BIN
+    if not os.path.exists(ref_bin):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/barbie_ref was not built (reference "
+                          "sources absent when building)"}), flush=True)
+        return
+    from barbie_b200.synth import realization_seed, synth_field, write_field
+    W = WORKLOAD
+    NN = W["NN"]
+    cores = os.cpu_count() or 1
+    scratch = os.path.join(ROOT, "_bench_ref")
+    os.makedirs(os.path.join(scratch, f"ResFiles_N{NN}", "data_files"), exist_ok=True)
+    field_path = os.path.join(scratch, f"field_N{NN}_R1.txt")
+    if not os.path.exists(field_path):
+        write_field(field_path, synth_field(NN, realization_seed(1)))
+    env = dict(os.environ, BEAM_REF_NMAX=str(W["Nmax"]), BEAM_REF_NR=str(W["Nr"]))
+
+    def ref_cmd(p1lo, p1hi, rplo, rphi):
+        e = dict(env, BEAM_REF_P1_LO=str(p1lo), BEAM_REF_P1_HI=str(p1hi), BEAM_REF_RP_LO=str(rplo),
+                 BEAM_REF_RP_HI=str(rphi))
+        args_ = f"ulimit -s unlimited; exec {ref_bin} {NN} 1 {W['UL_k1']} {W['LL_k1']} {W['BW_k1']}"
+        return ["bash", "-c", args_], e
+
+    # set-up: the reference's own caches (closed_rings_<NN> and the plane-ring files)
+    cmd, e = ref_cmd(0, 0, 0, 0)
+    t0 = time.perf_counter()
+    out = subprocess.run(cmd, cwd=scratch, env=e, capture_output=True, text=True)
+    t_setup = time.perf_counter() - t0
+    m = re.search(r"4\. Calculation done successfully \(in ([0-9.]+) sec\)", out.stdout)
+    t_cache = float(m.group(1)) if m else t_setup
+    m = re.search(r"2\. Calculation of ring combinations completed successfully \(in ([0-9.]+) sec\)", out.stdout)
+    t_calcr = float(m.group(1)) if m else 0.0
+
+    # samples: consecutive ring triplets of one p1, about `target` accepted triangles each
+    rings = oracle_py.closed_rings(NN, W["Nr"], W["Nmax"])
+    tri, _ = oracle_py.enumerate_triples(NN, W["Nmax"], W["Nr"], W["UL_k1"], W["LL_k1"], W["BW_k1"], rings4=rings)
+    ntri = len(tri)
+    nproc = max(1, min(cores, 64))
+    target = 4000
+    samples = []
+    for k in range(nproc * max(1, args.steps + args.warmup)):
+        p1 = 1 + (7 * k) % 49
+        sel = tri["rp"][tri["p1"] == p1]
+        counts = np.bincount(sel, minlength=len(rings))
+        start = (k * 131) % max(1, len(rings) - 1)
+        acc, end = 0, start
+        while end < len(rings) and acc < target:
+            acc += counts[end]
+            end += 1
+        samples.append((p1, start, end, int(acc)))
+
+    def step(k0):
+        procs = []
+        for j in range(nproc):
+            p1, a, b, n = samples[(k0 * nproc + j) % len(samples)]
+            cmd, e = ref_cmd(p1, p1 + 1, a, b)
+            procs.append((subprocess.Popen(cmd, cwd=scratch, env=e, stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                           text=True), n))
+        rates = []
+        for pr, n in procs:
+            o, _ = pr.communicate()
+            m = re.search(r"Total time ([0-9.]+)", o)
+            if m and float(m.group(1)) > 0 and n > 0:
+                rates.append(n / float(m.group(1)))
+        return rates
+
+    for k in range(args.warmup):
+        step(k)
+    vals, per_tri = [], []
+    for k in range(args.steps):
+        rates = step(args.warmup + k)
+        # each process is one realization stream: per bispectrum the loop over all
+        # accepted triangles plus the cache build it needs
+        per = [ntri / r + t_cache + t_calcr for r in rates]
+        vals.append(sum(3600.0 / s for s in per))
+        per_tri.extend(1.0 / r for r in rates)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, **W},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": "reference",
+                             "sample": f"{nproc} concurrent reference processes per step, each the triangle loop "
+                                       f"of one p1 over a window of ring triplets (~{target} accepted triangles); "
+                                       f"extrapolated to {ntri} triangles plus the measured cache build "
+                                       f"({t_cache:.1f} s) and calCR ({t_calcr:.1f} s)",
+                             "seconds_per_triangle": float(np.median(per_tri)) if per_tri else None},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
