@@ -404,7 +404,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   }
   for (int n = 0; n <= TRI_WARPS; ++n) d.class_first[n + 1] += d.class_first[n];
   for (int n = 1; n <= TRI_WARPS; ++n)
-    if ((size_t)TRI_STAGES * d.class_stage[n] * elem + sizeof(double) * TRI_P1 * 32 * n > budget) {
+    if ((size_t)TRI_STAGES * d.class_stage[n] * elem > budget) {
       set_detail("staged mode rows do not fit shared memory");
       return BEAM_EINVAL;
     }

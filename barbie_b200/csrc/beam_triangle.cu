@@ -146,11 +146,9 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
   const int ox0 = tl.p1_0 + a.colbase - it.colx;                          // x reads ox0 + q
   const int oz = any ? p3 + a.colbase - it.colz : 0;                      // z read
   const int oy0 = any ? -tl.p1_0 - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
-  // per-thread sums in shared memory ([q][thread]): they change once per piece
-  double *sum = reinterpret_cast<double *>(smem_raw + (size_t)TRI_STAGES * a.stage * sizeof(C)) + tid;
-  const int sstride = 32 * ncons;
+  double sum[TRI_P1];
 #pragma unroll
-  for (int q = 0; q < TRI_P1; ++q) sum[q * sstride] = 0.0;
+  for (int q = 0; q < TRI_P1; ++q) sum[q] = 0.0;
 
   int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
   for (int c = 0; c < nch; ++c) {
@@ -175,18 +173,24 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
       for (int j = 0; j < len; ++j, ++tt) {
         const C z = zs[tt * it.Lz + oz];
         const C *xr = xs + tt * it.Lx + ox0;
+        // x in two halves: the empty asm keeps the compiler from holding all
+        // TRI_P1 values at once, which leaves the sums room in registers
 #pragma unroll
-        for (int q = 0; q < TRI_P1; ++q) {
-          const C x = xr[q];
-          wr[q] = fma(x.x, z.x, fma(-x.y, z.y, wr[q]));
-          wi[q] = fma(x.x, z.y, fma(x.y, z.x, wi[q]));
+        for (int h = 0; h < TRI_P1; h += TRI_P1 / 2) {
+#pragma unroll
+          for (int q = h; q < h + TRI_P1 / 2; ++q) {
+            const C x = xr[q];
+            wr[q] = fma(x.x, z.x, fma(-x.y, z.y, wr[q]));
+            wi[q] = fma(x.x, z.y, fma(x.y, z.x, wi[q]));
+          }
+          asm volatile("" ::: "memory");
         }
       }
       const C *yr = ys + pc * it.Ly + oy0;
 #pragma unroll
       for (int q = 0; q < TRI_P1; ++q) {
         const C y = yr[-q];
-        sum[q * sstride] += (double)fma(y.x, wr[q], -y.y * wi[q]);
+        sum[q] += (double)fma(y.x, wr[q], -y.y * wi[q]);
       }
     }
     __syncwarp();
@@ -197,7 +201,7 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
 #pragma unroll
   for (int q = 0; q < TRI_P1; ++q) {
     const int cidx = tc[q * 32];
-    if (cidx >= 0) out[cidx] = sum[q * sstride];
+    if (cidx >= 0) out[cidx] = sum[q];
   }
 }
 
@@ -219,7 +223,8 @@ __global__ void k_reduce(long long n_combo, const int32_t *__restrict__ combo_u,
 
 template <typename C>
 static size_t tri_smem(int stage, int ntiles) {
-  return (size_t)TRI_STAGES * stage * sizeof(C) + sizeof(double) * TRI_P1 * 32 * ntiles;
+  (void)ntiles;
+  return (size_t)TRI_STAGES * stage * sizeof(C);
 }
 
 // One launch per tile count n (CTAs of n consumer warps + 1 producer warp), on

@@ -137,12 +137,12 @@ def measured_fp64_peak(torch, device) -> float:
 
 def profile_traffic(kernel: str):
     """DRAM bytes per launch of a kernel from a committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_nn384.txt")
+    path = os.path.join(ROOT, "profiles", f"{kernel}_nn384.md")
     if not os.path.exists(path):
         return None
     with open(path) as fh:
         for line in fh:
-            m = re.match(r"\s*dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", line)
+            m = re.search(r"dram_bytes_per_launch\s*=\s*([0-9.eE+]+)", line)
             if m:
                 return float(m.group(1))
     return None
