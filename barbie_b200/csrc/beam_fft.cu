@@ -17,6 +17,8 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <string>
 
 #include "beam_internal.h"
 
@@ -426,4 +428,159 @@ void free_pixel_path(beam_gpu_plan *p) {
   delete px;
 }
 
+// ----------------------------------------------- allocation-free plane rings
+// beam_gpu_plane_rings_noalloc: the same transform kernel, with its tables in
+// a fixed scratch array of the library's device image instead of cudaMalloc'd
+// buffers. The tables are assembled in a static host buffer (one call at a
+// time, under a mutex), copied into the scratch array on the caller's stream
+// and read by the kernel from there.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[BEAM_NOALLOC_SCRATCH_BYTES];
+alignas(16) static unsigned char g_noalloc_host[BEAM_NOALLOC_SCRATCH_BYTES];
+static std::mutex g_noalloc_mutex;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static void *g_noalloc_addr[NOALLOC_MAX_DEVICES];  // device address of the scratch array, per device
+
+// Device address of the scratch array on the current device, looked up once
+// per device (with that device current).
+static int noalloc_scratch(int dev, void **ptr) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+    set_detail("device ordinal beyond the allocation-free path's table");
+    return BEAM_EINVAL;
+  }
+  if (!g_noalloc_addr[dev]) {
+    void *a = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+    if (e != cudaSuccess || !a) {
+      set_detail(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+      return BEAM_ECUDA;
+    }
+    g_noalloc_addr[dev] = a;
+  }
+  *ptr = g_noalloc_addr[dev];
+  return BEAM_OK;
+}
+
+static size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
 }  // namespace beam
+
+extern "C" int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const double *r2c_dev, const int *planes,
+                                            const int *rings, int n, double *out_dev, void *stream) {
+  using namespace beam;
+  if (NN < 4 || NN % 2 || NN > 4096 || Nmax < 1 || Nmax > NN / 2 || Nr < 10 || Nr % 10 || Nr > 1000 || n < 0 ||
+      (n > 0 && (!r2c_dev || !planes || !rings || !out_dev))) {
+    set_detail("invalid arguments (NN even, 1 <= Nmax <= NN/2, Nr a multiple of 10, device buffers)");
+    return BEAM_EINVAL;
+  }
+  if (n > BEAM_NOALLOC_MAX_JOBS) {
+    set_detail("more than BEAM_NOALLOC_MAX_JOBS (plane, ring) pairs in one call");
+    return BEAM_EINVAL;
+  }
+  for (int k = 0; k < n; ++k)
+    if (planes[k] < 0 || planes[k] >= Nmax || rings[k] < 0 || rings[k] >= Nr) {
+      set_detail("plane or ring out of range");
+      return BEAM_EINVAL;
+    }
+  if (n == 0) return BEAM_OK;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  int dev = 0;
+  BEAM_CUDA(cudaGetDevice(&dev));
+  void *scratch = nullptr;
+  BEAM_TRY(noalloc_scratch(dev, &scratch));
+
+  // ring edges and, for the requested rings, their non-zero rows and modes in
+  // row-major order (the order beam_gpu_plane_rings uses)
+  double low[1000], high[1000], avg[1000];
+  if (beam_ring_edges(Nr, Nmax, low, high, avg) != BEAM_OK) return BEAM_EINVAL;
+  bool want[1000] = {};
+  for (int k = 0; k < n; ++k) want[rings[k]] = true;
+  size_t off_tw = 0;
+  size_t off_jobs = align16(off_tw + sizeof(double2) * NN);
+  size_t off_rr = align16(off_jobs + sizeof(int32_t) * 2 * n);
+  size_t off_rows = align16(off_rr + sizeof(RingRows) * Nr);
+  unsigned char *h = g_noalloc_host;
+  // count rows and modes first, to lay the tables out and check the limit
+  long nrows = 0, nmodes = 0;
+  int max_rows = 1;
+  for (long r = 0; r < Nr; ++r) {
+    if (!want[r]) continue;
+    long rows = 0;
+    for (long i = 0; i < NN; ++i) {
+      int ia = (int)((i > NN / 2) ? (i - NN) : i);
+      bool row = false;
+      for (long j = 0; j < NN; ++j) {
+        int ja = (int)((j > NN / 2) ? (j - NN) : j);
+        double kk = sqrt(1. * (ia * ia + ja * ja));
+        if (kk >= low[r] && kk < high[r]) {
+          ++nmodes;
+          row = true;
+        }
+      }
+      rows += row;
+    }
+    nrows += rows;
+    max_rows = std::max(max_rows, (int)rows);
+  }
+  size_t off_rmode = align16(off_rows + sizeof(int32_t) * nrows);
+  size_t off_mode = align16(off_rmode + sizeof(int32_t) * (nrows + 1));
+  size_t total = align16(off_mode + sizeof(int16_t) * 2 * nmodes);
+  if (total > BEAM_NOALLOC_SCRATCH_BYTES) {
+    set_detail("the requested rings need " + std::to_string(total) + " bytes of tables; the allocation-free path holds " +
+               std::to_string((size_t)BEAM_NOALLOC_SCRATCH_BYTES));
+    return BEAM_EINVAL;
+  }
+  double2 *tw = reinterpret_cast<double2 *>(h + off_tw);
+  for (long k = 0; k < NN; ++k) {
+    double a = 2.0 * M_PI * (double)k / (double)NN;
+    tw[k] = make_double2(std::cos(a), std::sin(a));
+  }
+  int32_t *jp = reinterpret_cast<int32_t *>(h + off_jobs);
+  for (int k = 0; k < n; ++k) {
+    jp[k] = planes[k];
+    jp[n + k] = rings[k];
+  }
+  RingRows *rr = reinterpret_cast<RingRows *>(h + off_rr);
+  int32_t *row_i = reinterpret_cast<int32_t *>(h + off_rows);
+  int32_t *row_mode = reinterpret_cast<int32_t *>(h + off_rmode);
+  int16_t *mode_ij = reinterpret_cast<int16_t *>(h + off_mode);
+  long at_row = 0, at_mode = 0;
+  for (long r = 0; r < Nr; ++r) {
+    rr[r] = RingRows{(int)at_row, 0};
+    if (!want[r]) continue;
+    for (long i = 0; i < NN; ++i) {
+      int ia = (int)((i > NN / 2) ? (i - NN) : i);
+      bool row = false;
+      for (long j = 0; j < NN; ++j) {
+        int ja = (int)((j > NN / 2) ? (j - NN) : j);
+        double kk = sqrt(1. * (ia * ia + ja * ja));
+        if (!(kk >= low[r] && kk < high[r])) continue;
+        if (!row) {
+          row_i[at_row] = (int32_t)i;
+          row_mode[at_row] = (int32_t)at_mode;
+          ++at_row;
+          row = true;
+        }
+        mode_ij[2 * at_mode] = (int16_t)i;
+        mode_ij[2 * at_mode + 1] = (int16_t)j;
+        ++at_mode;
+      }
+    }
+    rr[r].n_rows = (int)at_row - rr[r].first_row;
+  }
+  row_mode[at_row] = (int32_t)at_mode;
+
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  unsigned char *d = static_cast<unsigned char *>(scratch);
+  BEAM_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, st));
+  size_t smem = sizeof(double2) * ((size_t)NN + (size_t)max_rows * PR_YB);
+  BEAM_CUDA(cudaFuncSetAttribute(k_plane_ring_dft<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid((unsigned)((NN + PR_YB - 1) / PR_YB), (unsigned)n);
+  k_plane_ring_dft<double2><<<grid, PR_THREADS, smem, st>>>(
+      reinterpret_cast<const double2 *>(r2c_dev), (int)NN, reinterpret_cast<const int32_t *>(d + off_jobs),
+      reinterpret_cast<const int32_t *>(d + off_jobs) + n, reinterpret_cast<const RingRows *>(d + off_rr),
+      reinterpret_cast<const int32_t *>(d + off_rows), reinterpret_cast<const int32_t *>(d + off_rmode),
+      reinterpret_cast<const int16_t *>(d + off_mode), reinterpret_cast<const double2 *>(d + off_tw),
+      reinterpret_cast<double2 *>(out_dev), (long long)NN * NN);
+  BEAM_CUDA(cudaGetLastError());
+  return BEAM_OK;
+}

@@ -142,6 +142,32 @@ BEAM_API int beam_gpu_closed_rings(beam_gpu_plan *plan, double *rings4, long cap
 BEAM_API int beam_gpu_plane_rings(beam_gpu_plan *plan, const double *r2c, int r2c_on_device,
                          const int *planes, const int *rings, int n, double *out, int out_on_device);
 
+/* Plane-ring transforms without any device allocation. It has no counterpart
+ * in the reference; it serves callers that must not call cudaMalloc: code that
+ * runs inside an application whose own allocator has already claimed the
+ * device memory, processes under a hard device-memory quota, and latency-
+ * sensitive loops where cudaMalloc's implicit device synchronisation is not
+ * acceptable.
+ * Same result as beam_gpu_plane_rings for the same inputs, but all buffers are
+ * the caller's: r2c_dev is the r2c buffer double[NN][NN][NN+2] in device
+ * memory, out_dev receives n arrays complex128[NN][NN] in device memory, and
+ * planes/rings are host arrays of n entries (0 <= plane < Nmax <= NN/2,
+ * 0 <= ring < Nr, Nr a multiple of 10). Work is queued on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) of the current device and
+ * the call returns without waiting for it.
+ * The ring tables, twiddles and job list go to a fixed scratch array of
+ * BEAM_NOALLOC_SCRATCH_BYTES in the library's device image; each GPU that
+ * loads the library holds that array until the process exits. A call whose
+ * tables need more (many rings or large NN), or n > BEAM_NOALLOC_MAX_JOBS,
+ * returns BEAM_EINVAL and explains in beam_gpu_last_error_detail(). The first
+ * call on a device looks the array's address up once (make that first call
+ * before any stream capture). Every call rewrites the array, so calls whose
+ * work overlaps on the GPU race on it: order them on one stream. */
+#define BEAM_NOALLOC_SCRATCH_BYTES (2u * 1024u * 1024u)
+#define BEAM_NOALLOC_MAX_JOBS 4096
+BEAM_API int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const double *r2c_dev, const int *planes,
+                                          const int *rings, int n, double *out_dev, void *stream);
+
 /* Per-triangle sums B (barbie.c:326-337, the value added at :360 before the bs
  * weight) for all accepted triangles in loop order, written to B (host, n_triples
  * doubles). The plan's method and precision apply. */
