@@ -196,8 +196,10 @@ static int upload(beam_gpu_plan *p, T **dst, const std::vector<T> &src) {
 
 // Tiles, pieces, chunks and CTA work items of the triangle-sum kernel.
 //  * tiles: per ring triplet, its combos (p1, p2) placed on a grid of
-//    TRI_P1 planes p1 x 32 planes p3 (p3 = -p1-p2); tiles are grouped four p1
-//    blocks by two p3 windows per CTA so the staged row segments stay short;
+//    TRI_P1 planes p1 x 32 planes p3 (p3 = -p1-p2); a CTA takes the tiles of
+//    one p3 window and up to TRI_WARPS consecutive p1 blocks, so it stages
+//    one z segment of 32 planes and x/y segments of at most
+//    TRI_WARPS * TRI_P1 + 32 planes;
 //  * runs: consecutive list entries sharing k2 (k2cnt, list order); a
 //    triplet's runs are split into `ns` contiguous ranges of about equal size
 //    when its work is large, so its CTAs share the triangle list;
