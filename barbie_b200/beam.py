@@ -51,7 +51,8 @@ class Cfg(ctypes.Structure):
     _fields_ = [("NN", ctypes.c_long), ("Nmax", ctypes.c_long), ("Nr", ctypes.c_long),
                 ("UL_k1", ctypes.c_int), ("LL_k1", ctypes.c_int), ("BW_k1", ctypes.c_int),
                 ("n_mtbin", ctypes.c_int), ("LL", ctypes.c_double),
-                ("precision", ctypes.c_int), ("method", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("method", ctypes.c_int),
+                ("shard_index", ctypes.c_int), ("shard_count", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -63,7 +64,9 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("n_k1bin", ctypes.c_int), ("n_bins", ctypes.c_long), ("n_closed_triplets", ctypes.c_long),
                 ("n_triples", ctypes.c_long), ("n_used_triplets", ctypes.c_long),
                 ("n_fourier_terms", ctypes.c_long), ("n_modes", ctypes.c_long), ("n_planes", ctypes.c_int),
-                ("device_bytes", ctypes.c_size_t), ("vol", ctypes.c_double)]
+                ("device_bytes", ctypes.c_size_t), ("vol", ctypes.c_double),
+                ("n_shard_terms", ctypes.c_long), ("launches_last_run", ctypes.c_int),
+                ("run_bytes", ctypes.c_size_t)]
 
 
 _lib = None
@@ -100,6 +103,8 @@ def load() -> ctypes.CDLL:
     L.beam_gpu_plan_get_info.argtypes = [vp, ctypes.POINTER(PlanInfo)]
     L.beam_gpu_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Result)]
     L.beam_gpu_run_batch.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(Result)]
+    L.beam_gpu_run_batch_ex.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(Result), ctypes.c_int]
+    L.beam_shard_assign.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.beam_gpu_closed_rings.argtypes = [vp, dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
     L.beam_gpu_plane_rings.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int), ctypes.c_int, vp, ctypes.c_int]
@@ -109,10 +114,21 @@ def load() -> ctypes.CDLL:
     L.beam_gpu_plan_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
     L.beam_gpu_plan_last_timings.restype = ctypes.c_int
     for name in ("beam_gpu_init", "beam_gpu_plan_create", "beam_gpu_plan_get_info", "beam_gpu_run",
-                 "beam_gpu_run_batch", "beam_gpu_closed_rings", "beam_gpu_plane_rings", "beam_gpu_triangle_sums"):
+                 "beam_gpu_run_batch", "beam_gpu_run_batch_ex", "beam_shard_assign", "beam_gpu_closed_rings",
+                 "beam_gpu_plane_rings", "beam_gpu_triangle_sums"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
+
+
+def shard_assign(work, shard_count: int) -> np.ndarray:
+    """Owner shard of each work unit (beam_shard_assign; host only, no GPU)."""
+    L = load()
+    w = np.ascontiguousarray(work, dtype=np.float64)
+    owner = np.zeros(max(1, w.size), dtype=np.int32)
+    _check(L.beam_shard_assign(w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), w.size, shard_count,
+                               owner.ctypes.data_as(ctypes.POINTER(ctypes.c_int))), "beam_shard_assign")
+    return owner[: w.size]
 
 
 def _check(rc: int, what: str) -> None:
@@ -170,12 +186,13 @@ class Plan:
 
     def __init__(self, ctx: Context, NN: int, UL_k1: int, LL_k1: int, BW_k1: int, *, Nmax: int = 100,
                  Nr: int = 40, n_mtbin: int = 5, LL: float = 1.0, precision: str = "fp64",
-                 method: str = "triangle"):
+                 method: str = "triangle", shard: tuple[int, int] = (0, 1)):
         L = load()
         cfg = Cfg()
         L.beam_cfg_default(ctypes.byref(cfg), NN, UL_k1, LL_k1, BW_k1)
         cfg.Nmax, cfg.Nr, cfg.n_mtbin, cfg.LL = Nmax, Nr, n_mtbin, LL
         cfg.precision, cfg.method = PREC[precision], METHOD[method]
+        cfg.shard_index, cfg.shard_count = shard
         h = ctypes.c_void_p()
         _check(L.beam_gpu_plan_create(ctx._h, ctypes.byref(cfg), ctypes.byref(h)), "beam_gpu_plan_create")
         self._h, self.ctx, self.cfg = h, ctx, cfg
@@ -215,8 +232,9 @@ class Plan:
         _check(_lib.beam_gpu_run(self._h, addr, dev, ctypes.byref(res)), "beam_gpu_run")
         return arrays
 
-    def run_batch(self, fields: list) -> list[dict]:
-        """Several realizations (host numpy arrays) through beam_gpu_run_batch."""
+    def run_batch(self, fields: list, batch: int = 0) -> list[dict]:
+        """Several realizations (host numpy arrays) through beam_gpu_run_batch_ex
+        (batch = realizations per device batch, 0 = chosen by the library)."""
         addrs = (ctypes.c_void_p * len(fields))()
         results = (Result * len(fields))()
         out = []
@@ -228,8 +246,15 @@ class Plan:
             addrs[k] = a
             results[k], arrays = self._result()
             out.append(arrays)
-        _check(_lib.beam_gpu_run_batch(self._h, addrs, len(fields), results), "beam_gpu_run_batch")
+        _check(_lib.beam_gpu_run_batch_ex(self._h, addrs, len(fields), results, batch), "beam_gpu_run_batch_ex")
         return out
+
+    def refresh_info(self) -> dict:
+        """Re-read beam_gpu_plan_get_info (device bytes and launch count change as the plan runs)."""
+        info = PlanInfo()
+        _check(_lib.beam_gpu_plan_get_info(self._h, ctypes.byref(info)), "beam_gpu_plan_get_info")
+        self.info = {k: getattr(info, k) for k, _ in PlanInfo._fields_}
+        return self.info
 
     def triangle_sums(self, r2c) -> np.ndarray:
         """B per accepted triangle in the reference's loop order."""

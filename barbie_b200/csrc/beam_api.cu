@@ -3,6 +3,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <thread>
 
 #include "beam_internal.h"
 
@@ -15,6 +16,7 @@ int pixel_triangle_sums(beam_gpu_plan *p, const double *r2c, int on_device);
 bool pixel_method(const beam_gpu_plan *p);
 int build_pixel_path(beam_gpu_plan *p);
 void free_pixel_path(beam_gpu_plan *p);
+int triangle_init_attributes(size_t smem_optin);
 }  // namespace beam
 
 using namespace beam;
@@ -33,6 +35,24 @@ void beam_cfg_default(beam_cfg *cfg, long NN, int UL_k1, int LL_k1, int BW_k1) {
   cfg->LL = 1.0;     // barbie.c:67
   cfg->precision = BEAM_PREC_FP64;
   cfg->method = BEAM_METHOD_TRIANGLE;
+  cfg->shard_index = 0;
+  cfg->shard_count = 1;
+}
+
+int beam_shard_assign(const double *work, int n, int shard_count, int *owner) {
+  if (n < 0 || shard_count < 1 || (n > 0 && (!work || !owner))) return BEAM_EINVAL;
+  std::vector<int> order(n);
+  for (int u = 0; u < n; ++u) order[u] = u;
+  std::stable_sort(order.begin(), order.end(), [work](int a, int b) { return work[a] > work[b]; });
+  std::vector<double> load(shard_count, 0.0);
+  for (int u : order) {
+    int best = 0;
+    for (int k = 1; k < shard_count; ++k)
+      if (load[k] < load[best]) best = k;
+    owner[u] = best;
+    load[best] += work[u];
+  }
+  return BEAM_OK;
 }
 
 const char *beam_gpu_strerror(int code) {
@@ -74,17 +94,13 @@ int beam_gpu_init(int device, beam_gpu_ctx **out) {
   c->device = device;
   c->num_sms = prop.multiProcessorCount;
   c->smem_optin = prop.sharedMemPerBlockOptin;
-  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-  for (int k = 0; k < TRI_WARPS && e == cudaSuccess; ++k) {
-    e = cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->join[k], cudaEventDisableTiming);
-  }
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
-  if (e != cudaSuccess) {
-    set_detail(cudaGetErrorString(e));
+  int rc = lane_create(&c->lane);
+  if (rc == BEAM_OK) rc = triangle_init_attributes(c->smem_optin);
+  if (rc != BEAM_OK) {
     beam_gpu_destroy(c);
-    return BEAM_ECUDA;
+    return rc;
   }
+  c->stream = c->lane.stream;
   *out = c;
   return BEAM_OK;
 }
@@ -92,12 +108,7 @@ int beam_gpu_init(int device, beam_gpu_ctx **out) {
 void beam_gpu_destroy(beam_gpu_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
-  for (int k = 0; k < TRI_WARPS; ++k) {
-    if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
-    if (ctx->join[k]) cudaEventDestroy(ctx->join[k]);
-  }
-  if (ctx->fork) cudaEventDestroy(ctx->fork);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  lane_destroy(&ctx->lane);
   delete ctx;
 }
 
@@ -109,19 +120,24 @@ int beam_gpu_plan_create(beam_gpu_ctx *ctx, const beam_cfg *cfg, beam_gpu_plan *
     set_detail("unknown precision or method");
     return BEAM_EINVAL;
   }
+  const int shards = cfg->shard_count < 1 ? 1 : cfg->shard_count;
+  if (cfg->shard_index < 0 || cfg->shard_index >= shards || (shards > 1 && cfg->method != BEAM_METHOD_TRIANGLE)) {
+    set_detail("shard_index must lie in [0, shard_count); sharding needs the triangle method");
+    return BEAM_EINVAL;
+  }
   BEAM_CUDA(cudaSetDevice(ctx->device));
   beam_gpu_plan *p = new (std::nothrow) beam_gpu_plan();
   if (!p) return BEAM_ENOMEM;
   p->ctx = ctx;
   p->cfg = *cfg;
+  p->cfg.shard_count = shards;
   int rc = beam_geom_build(&p->geom, cfg);
   if (rc == BEAM_EBOUNDS) set_detail("a triangle's (k1, t, mu) bin falls outside the bin arrays");
   if (rc == BEAM_EINVAL) set_detail("invalid configuration (NN even, Nmax <= NN/2, Nr a multiple of 10, "
                                     "BW_k1 > 0 dividing UL_k1 - LL_k1 > 0)");
   if (rc == BEAM_OK) rc = build_plan_tables(p);
+  if (rc == BEAM_OK) rc = slot_create(p, 1, &ctx->lane, &p->main);
   if (rc == BEAM_OK && pixel_method(p)) rc = build_pixel_path(p);
-  for (int k = 0; k < 5 && rc == BEAM_OK; ++k)
-    if (cudaEventCreate(&p->ev[k]) != cudaSuccess) rc = BEAM_ECUDA;
   if (rc != BEAM_OK) {
     beam_gpu_plan_destroy(p);
     return rc;
@@ -134,8 +150,12 @@ void beam_gpu_plan_destroy(beam_gpu_plan *p) {
   if (!p) return;
   cudaSetDevice(p->ctx->device);
   cudaStreamSynchronize(p->ctx->stream);
-  for (int k = 0; k < 5; ++k)
-    if (p->ev[k]) cudaEventDestroy(p->ev[k]);
+  for (beam::RunSlot *&s : p->batch) {
+    slot_destroy(s);
+    s = nullptr;
+  }
+  slot_destroy(p->main);
+  p->main = nullptr;
   free_pixel_path(p);
   free_plan_tables(p);
   beam_geom_free(&p->geom);
@@ -158,69 +178,144 @@ int beam_gpu_plan_get_info(const beam_gpu_plan *p, beam_plan_info *info) {
   for (size_t u = 0; u < p->used_rp.size(); ++u) u_of_rp[p->used_rp[u]] = (int)u;
   for (long long t = 0; t < p->geom.ntri; ++t) terms += per_u[u_of_rp[p->geom.t_rp[t]]];
   info->n_fourier_terms = terms;
+  long long mine = terms;
+  if (p->cfg.shard_count > 1) {
+    mine = 0;
+    for (long long t = 0; t < p->geom.ntri; ++t) {
+      int u = u_of_rp[p->geom.t_rp[t]];
+      if (p->u_owner[u] == p->cfg.shard_index) mine += per_u[u];
+    }
+  }
+  info->n_shard_terms = mine;
   info->n_modes = p->d.n_modes;
   info->n_planes = p->d.Q;
-  info->device_bytes = p->device_bytes;
+  size_t bytes = p->device_bytes + (p->main ? p->main->bytes : 0);
+  for (const RunSlot *s : p->batch) bytes += s ? s->bytes : 0;
+  info->device_bytes = bytes;
   info->vol = p->geom.vol;
+  info->launches_last_run = p->main ? p->main->launches : 0;
+  info->run_bytes = slot_bytes(p, 1);
   return BEAM_OK;
 }
 
-static int copy_results(beam_gpu_plan *p, beam_result *res) {
-  DevPlan &d = p->d;
-  cudaStream_t s = p->ctx->stream;
-  size_t nb = (size_t)d.n_bins;
-  if (nb) {
-    BEAM_CUDA(cudaMemcpyAsync(p->h_bins, d.bins, sizeof(double) * 3 * nb * BEAM_NPOLES, cudaMemcpyDeviceToHost, s));
-    BEAM_CUDA(cudaMemcpyAsync(p->h_count, d.bin_count, sizeof(long long) * nb, cudaMemcpyDeviceToHost, s));
-  }
-  BEAM_TRY(check_status(p));  // synchronizes the stream
-  if (!res) return BEAM_OK;
-  size_t n = nb * BEAM_NPOLES;
-  if (res->bs) std::memcpy(res->bs, p->h_bins, sizeof(double) * n);
-  if (res->norm) std::memcpy(res->norm, p->h_bins + n, sizeof(double) * n);
-  if (res->out) std::memcpy(res->out, p->h_bins + 2 * n, sizeof(double) * n);
-  if (res->count)
-    for (size_t b = 0; b < nb; ++b) res->count[b] = (int64_t)p->h_count[b];
-  return BEAM_OK;
-}
-
+// Triangle sums of one realization on the plan's own slot.
 static int compute_B(beam_gpu_plan *p, const double *r2c, int on_device) {
-  p->timed = false;
-  mark(p, 0);
+  RunSlot *s = p->main;
+  s->timed = false;
+  s->launches = 0;
+  mark(s, 0);
   if (pixel_method(p)) return pixel_triangle_sums(p, r2c, on_device);
-  if (on_device)
-    BEAM_TRY(upload_modes_device(p, r2c));
-  else
-    BEAM_TRY(upload_modes_host(p, r2c));
-  return run_triangle_sums(p);
+  if (on_device) {
+    s->h_src[s->cap] = r2c;
+    BEAM_TRY(upload_modes(p, s, 1, false));
+  } else {
+    gather_host(p, s, 0, r2c);
+    BEAM_TRY(upload_modes(p, s, 1, true));
+  }
+  return run_triangle_sums(p, s, 1);
 }
 
 int beam_gpu_run(beam_gpu_plan *p, const double *r2c, int r2c_on_device, beam_result *res) {
   if (!p || !r2c) return BEAM_EINVAL;
   BEAM_CUDA(cudaSetDevice(p->ctx->device));
+  RunSlot *s = p->main;
   BEAM_TRY(compute_B(p, r2c, r2c_on_device));
-  BEAM_TRY(run_epilogue(p));
-  mark(p, 4);
-  p->timed = true;
-  return copy_results(p, res);
+  BEAM_TRY(run_epilogue(p, s, 1));
+  mark(s, 4);
+  BEAM_TRY(fetch_results(p, s, 1));
+  BEAM_TRY(check_status(s));
+  s->timed = true;
+  return copy_result(p, s, 0, res);
+}
+
+// Copy the mode rows of realizations r2c[0..n) into slot rows [0, n), split
+// over a few host threads.
+static void gather_batch(const beam_gpu_plan *p, RunSlot *s, const double *const *r2c, int n) {
+  unsigned hw = std::thread::hardware_concurrency();
+  int nt = (int)std::min<unsigned>(std::max(1u, hw), 8u);
+  nt = std::min(nt, n);
+  if (nt <= 1) {
+    for (int r = 0; r < n; ++r) gather_host(p, s, r, r2c[r]);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int k = 0; k < nt; ++k)
+    th.emplace_back([=]() {
+      for (int r = k; r < n; r += nt) gather_host(p, s, r, r2c[r]);
+    });
+  for (std::thread &t : th) t.join();
+}
+
+int beam_gpu_run_batch_ex(beam_gpu_plan *p, const double *const *r2c, int n, beam_result *res, int batch) {
+  if (!p || (!r2c && n > 0) || n < 0 || batch < 0) return BEAM_EINVAL;
+  for (int i = 0; i < n; ++i)
+    if (!r2c[i]) return BEAM_EINVAL;
+  if (n == 0) return BEAM_OK;
+  BEAM_CUDA(cudaSetDevice(p->ctx->device));
+  if (pixel_method(p)) {
+    for (int i = 0; i < n; ++i) BEAM_TRY(beam_gpu_run(p, r2c[i], 0, res ? &res[i] : nullptr));
+    return BEAM_OK;
+  }
+  int b = batch;
+  if (b == 0) {
+    size_t fr = 0, tot = 0;
+    BEAM_CUDA(cudaMemGetInfo(&fr, &tot));
+    size_t per = std::max<size_t>(1, slot_bytes(p, 1));
+    b = (int)std::min<size_t>(64, std::max<size_t>(1, fr / 4 / per));  // two slots in half the free memory
+  }
+  b = std::min(std::min(b, n), 65535);
+  const int nslots = n > b ? 2 : 1;
+  for (int k = 0; k < nslots; ++k)
+    if (!p->batch[k] || p->batch[k]->cap < b) {
+      slot_destroy(p->batch[k]);
+      p->batch[k] = nullptr;
+      BEAM_TRY(slot_create(p, b, nullptr, &p->batch[k]));
+    }
+  int first[2] = {-1, -1}, count[2] = {0, 0};
+  int rc = BEAM_OK;
+  auto retire = [&](int k) {
+    if (first[k] < 0) return BEAM_OK;
+    int r = check_status(p->batch[k]);
+    for (int j = 0; j < count[k] && r == BEAM_OK && res; ++j) copy_result(p, p->batch[k], j, &res[first[k] + j]);
+    first[k] = -1;
+    return r;
+  };
+  for (int i = 0, r0 = 0; r0 < n && rc == BEAM_OK; ++i, r0 += b) {
+    const int k = i % nslots, nb = std::min(b, n - r0);
+    rc = retire(k);  // the slot's previous batch has finished: its staging rows may be rewritten
+    if (rc != BEAM_OK) break;
+    gather_batch(p, p->batch[k], r2c + r0, nb);
+    rc = slot_run_graph(p, p->batch[k], nb);
+    if (rc == BEAM_OK) {
+      first[k] = r0;
+      count[k] = nb;
+    }
+  }
+  for (int k = 0; k < nslots; ++k) {
+    int r = retire(k);
+    if (rc == BEAM_OK) rc = r;
+  }
+  return rc;
 }
 
 int beam_gpu_run_batch(beam_gpu_plan *p, const double *const *r2c, int n, beam_result *res) {
-  if (!p || (!r2c && n > 0) || n < 0) return BEAM_EINVAL;
-  for (int i = 0; i < n; ++i) BEAM_TRY(beam_gpu_run(p, r2c[i], 0, res ? &res[i] : nullptr));
-  return BEAM_OK;
+  return beam_gpu_run_batch_ex(p, r2c, n, res, 0);
 }
 
 int beam_gpu_triangle_sums(beam_gpu_plan *p, const double *r2c, int r2c_on_device, double *B) {
   if (!p || !r2c || !B) return BEAM_EINVAL;
   BEAM_CUDA(cudaSetDevice(p->ctx->device));
+  RunSlot *s = p->main;
   BEAM_TRY(compute_B(p, r2c, r2c_on_device));
-  mark(p, 4);
-  p->timed = true;
+  mark(s, 4);
   long long n = p->geom.ntri;
   std::vector<double> tmp((size_t)std::max<long long>(1, n));
-  if (n) BEAM_CUDA(cudaMemcpyAsync(tmp.data(), p->d.B, sizeof(double) * n, cudaMemcpyDeviceToHost, p->ctx->stream));
-  BEAM_TRY(check_status(p));
+  cudaStream_t st = s->lane->stream;
+  if (n) BEAM_CUDA(cudaMemcpyAsync(tmp.data(), s->B, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  BEAM_CUDA(cudaMemcpyAsync(s->h_status, s->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BEAM_CUDA(cudaEventRecord(s->done, st));
+  BEAM_TRY(check_status(s));
+  s->timed = true;
   for (long long i = 0; i < n; ++i) B[p->loop_of_bin[i]] = tmp[i];
   return BEAM_OK;
 }
@@ -252,9 +347,10 @@ void *beam_gpu_stream(beam_gpu_ctx *ctx) { return ctx ? (void *)ctx->stream : nu
 
 int beam_gpu_plan_last_timings(const beam_gpu_plan *p, float *ms, int n) {
   if (!p || !ms || n < 0) return BEAM_EINVAL;
-  if (!p->timed) return BEAM_EINVAL;
-  BEAM_CUDA(cudaEventSynchronize(p->ev[4]));
-  for (int k = 0; k < n && k < 4; ++k) BEAM_CUDA(cudaEventElapsedTime(&ms[k], p->ev[k], p->ev[k + 1]));
+  const RunSlot *s = p->main;
+  if (!s || !s->timed) return BEAM_EINVAL;
+  BEAM_CUDA(cudaEventSynchronize(s->ev[4]));
+  for (int k = 0; k < n && k < 4; ++k) BEAM_CUDA(cudaEventElapsedTime(&ms[k], s->ev[k], s->ev[k + 1]));
   return BEAM_OK;
 }
 

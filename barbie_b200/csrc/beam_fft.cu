@@ -398,21 +398,24 @@ int pixel_triangle_sums(beam_gpu_plan *p, const double *r2c, int on_device) {
     BEAM_CUDA(cudaMemcpyAsync(px->r2c, r2c, sizeof(double) * NN * NN * (NN + 2), cudaMemcpyHostToDevice, s));
     src = px->r2c;
   }
+  RunSlot *slot = p->main;
   BEAM_TRY(launch_dft<double2>(p, px, src, px->slot_plane, px->slot_ring, px->n_slots, (double2 *)px->cache, n2));
-  mark(p, 1);
+  slot->launches += (px->n_slots + 65534) / 65535;
+  mark(slot, 1);
   if (px->n_pairs == 0) {
-    mark(p, 2);
-    mark(p, 3);
+    mark(slot, 2);
+    mark(slot, 3);
     return BEAM_OK;
   }
   size_t smem = sizeof(double2) * (size_t)px->max_pair_rows * px->xtile;
   BEAM_CUDA(cudaFuncSetAttribute(k_pixel_sums, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_pixel_sums<<<px->n_pairs, PIX_THREADS, smem, s>>>((const double2 *)px->cache, n2, px->xtile, px->pair_first,
                                                       px->pair_row_first, px->pair_rows, px->tri_rows, px->tri_sign,
-                                                      px->tri_out, p->d.B);
+                                                      px->tri_out, slot->B);
   BEAM_CUDA(cudaGetLastError());
-  mark(p, 2);
-  mark(p, 3);
+  slot->launches++;
+  mark(slot, 2);
+  mark(slot, 3);
   return BEAM_OK;
 }
 

@@ -92,7 +92,8 @@ struct TriItem {
   int colx, Lx, colz, Lz, coly, Ly;
 };
 
-// Device-side tables and buffers of a plan.
+// Device-side tables of a plan (read-only while it runs; per-run buffers live
+// in RunSlot).
 struct DevPlan {
   // ring modes on the planes in use
   // A mode's row holds planes q = -(Q-1)..Q-1 at columns colbase + q, with
@@ -126,33 +127,63 @@ struct DevPlan {
   TriItem *items = nullptr;       // [n_items]: grouped by tile count, largest work first in a group
   int class_first[TRI_WARPS + 2] = {};  // items with n tiles: [class_first[n], class_first[n+1])
   int class_stage[TRI_WARPS + 1] = {};  // stage size (complex values) of the CTAs with n tiles
-  long long n_part = 0;
-  double *part = nullptr;         // [n_part] partial sums
-  // per-realization buffers
-  double *staging = nullptr;      // [n_modes][Q] complex128 rows of the r2c buffer
-  double *S64 = nullptr;          // [n_modes][W] complex128 signed-plane mode data
-  float *S32 = nullptr;           // [n_modes][W] complex64 (mixed precision)
-  double *B = nullptr;            // [n_combo] triangle sums, bin order
+  long long n_part = 0;           // partial-sum slots per realization
+  size_t elem = 0;                // bytes of one complex mode value (16 FP64, 8 mixed)
   // epilogue (bin order)
   int n_bins = 0;
   int32_t *bin_first = nullptr;   // [n_bins+1]
   double *ep_px = nullptr, *ep_pz = nullptr;  // [n_combo]
   int32_t *ep_cnt = nullptr;      // [n_combo] exact in-plane triangle count
-  double *bins = nullptr;         // [3][n_bins][16]: bs, norm, out
-  long long *bin_count = nullptr; // [n_bins]
+};
+
+// A stream plus the side streams the per-class triangle-sum launches fork onto.
+struct Lane {
+  cudaStream_t stream = nullptr;
+  cudaStream_t side[TRI_WARPS] = {};
+  cudaEvent_t fork = nullptr, join[TRI_WARPS] = {};
+};
+int lane_create(Lane *l);
+void lane_destroy(Lane *l);
+
+// Per-run buffers for up to `cap` realizations of one plan, processed together
+// (realization r of a launch is its blockIdx.y). The plan's own slot (cap 1)
+// serves beam_gpu_run; batches and the job server create more. All device
+// buffers are realization-major.
+struct RunSlot {
+  int cap = 0;
+  Lane *lane = nullptr;           // where the slot's work is queued
+  Lane own;                       // used when the slot has a lane of its own
+  double *staging = nullptr;      // [cap][n_modes][Q] complex128 rows of the r2c buffers
+  const double **src = nullptr;   // [2*cap] device: staged rows per realization, then device r2c buffers
+  const double **h_src = nullptr; // [2*cap] pinned mirror of src
+  void *S = nullptr;              // [cap][n_modes][W] complex mode data (double2 or float2)
+  double *part = nullptr;         // [cap][n_part] partial sums (zero where never written)
+  double *B = nullptr;            // [cap][n_combo] triangle sums, bin order
+  double *bins = nullptr;         // [cap][3][n_bins][16]: bs, norm, out
+  long long *bin_count = nullptr; // [cap][n_bins]
   int *status = nullptr;          // device status word
+  double *h_staging = nullptr;    // pinned [cap][n_modes][Q]
+  double *h_bins = nullptr;       // pinned [cap][3][n_bins][16]
+  long long *h_count = nullptr;   // pinned [cap][n_bins]
+  int *h_status = nullptr;        // pinned status copy
+  cudaEvent_t ev[5] = {};         // stage boundaries (beam_gpu_plan_last_timings)
+  cudaEvent_t done = nullptr;     // end of the last queued run
+  bool timed = false;
+  bool capturing = false;         // inside slot_run_graph's stream capture (no stage marks)
+  int launches = 0;               // kernels launched by the last queued run
+  cudaGraphExec_t graph = nullptr;  // captured host-input run of graph_n realizations
+  int graph_n = 0;
+  size_t bytes = 0;               // device bytes of the slot
 };
 
 }  // namespace beam
 
 struct beam_gpu_ctx {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // == lane.stream
   int num_sms = 0;
   size_t smem_optin = 0;
-  // side streams forked from `stream` for the per-class triangle-sum launches
-  cudaStream_t side[beam::TRI_WARPS] = {};
-  cudaEvent_t fork = nullptr, join[beam::TRI_WARPS] = {};
+  beam::Lane lane;
 };
 
 struct beam_gpu_plan {
@@ -167,39 +198,48 @@ struct beam_gpu_plan {
   std::vector<int16_t> mode_ij;          // [n_modes][2]
   std::vector<int32_t> bin_pos;          // [ntri] loop order -> bin order
   std::vector<int32_t> loop_of_bin;      // [ntri] bin order -> loop order
-  double *h_staging = nullptr;           // pinned [n_modes][Q] complex128
-  double *h_bins = nullptr;              // pinned [3][n_bins][16]
-  long long *h_count = nullptr;          // pinned [n_bins]
-  size_t device_bytes = 0;
+  std::vector<int> u_owner;              // [n_used] shard that sums each used ring triplet
+  size_t device_bytes = 0;               // tables (slots count separately)
   beam::PixelPath *pix = nullptr;        // plane-ring transform tables / pixel method
-  cudaEvent_t ev[5] = {};                // stage boundaries of the last run (beam_gpu_plan_last_timings)
-  bool timed = false;
+  beam::RunSlot *main = nullptr;         // slot of beam_gpu_run and friends (ctx->lane)
+  beam::RunSlot *batch[2] = {};          // double-buffered slots of beam_gpu_run_batch
 };
 
 namespace beam {
-// stage boundary k of the current run, on the context's stream
-inline void mark(beam_gpu_plan *p, int k) {
-  if (p->ev[k]) cudaEventRecord(p->ev[k], p->ctx->stream);
+// stage boundary k of the slot's current run, on its stream
+inline void mark(RunSlot *s, int k) {
+  if (s->ev[k] && !s->capturing) cudaEventRecord(s->ev[k], s->lane->stream);
 }
 // plan construction (beam_plan.cu)
 int build_plan_tables(beam_gpu_plan *p);
 void free_plan_tables(beam_gpu_plan *p);
 int count_closed_triangles(beam_gpu_plan *p, std::vector<long long> &counts);
-// per-realization steps (beam_run.cu)
-int upload_modes_host(beam_gpu_plan *p, const double *r2c);
-int upload_modes_device(beam_gpu_plan *p, const double *r2c_dev);
-int run_triangle_sums(beam_gpu_plan *p);
-int run_epilogue(beam_gpu_plan *p);
-int check_status(beam_gpu_plan *p);
+// run slots (beam_run.cu); lane == nullptr gives the slot a lane of its own
+size_t slot_bytes(const beam_gpu_plan *p, int cap);
+int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out);
+void slot_destroy(RunSlot *s);
+// per-realization steps on a slot, for realizations [0, n) (beam_run.cu)
+void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c);
+int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged);
+int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n);
+int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n);
+int fetch_results(beam_gpu_plan *p, RunSlot *s, int n);
+int check_status(RunSlot *s);
+int slot_run_graph(beam_gpu_plan *p, RunSlot *s, int n);
+int copy_result(const beam_gpu_plan *p, const RunSlot *s, int r, beam_result *res);
 template <typename T>
-int dev_alloc(beam_gpu_plan *p, T **ptr, size_t count) {
+int dev_alloc(size_t *total, T **ptr, size_t count) {
   size_t bytes = sizeof(T) * (count ? count : 1);
   cudaError_t e = cudaMalloc((void **)ptr, bytes);
   if (e != cudaSuccess) {
     set_detail(std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
     return BEAM_EDEVMEM;
   }
-  p->device_bytes += bytes;
+  *total += bytes;
   return BEAM_OK;
+}
+template <typename T>
+int dev_alloc(beam_gpu_plan *p, T **ptr, size_t count) {
+  return dev_alloc(&p->device_bytes, ptr, count);
 }
 }  // namespace beam

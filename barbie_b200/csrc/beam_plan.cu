@@ -206,11 +206,13 @@ static int upload(beam_gpu_plan *p, T **dst, const std::vector<T> &src) {
 //  * pieces: runs cut to at most TRI_CHUNK triangles; chunks: whole pieces
 //    packed up to TRI_CHUNK triangles.
 // A = 16-byte unit of complex values (1 or 2); u_part receives the first
-// partial-sum slot of each triplet (ns_u * ncombo_u slots each).
+// partial-sum slot of each triplet (ns_u * ncombo_u slots each). Triplets
+// that another shard sums (own[u] == 0) get no tiles, chunks or items and one
+// split of partial sums that stay zero, so their triangles come out as B = 0.
 static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, const std::vector<int32_t> &u_ncombo,
                       const std::vector<int32_t> &combo_p1, const std::vector<int32_t> &combo_p2,
-                      const std::vector<int> &k2cnt, int A, std::vector<int32_t> &u_nsplit,
-                      std::vector<long long> &u_part) {
+                      const std::vector<int> &k2cnt, const std::vector<char> &own, int A,
+                      std::vector<int32_t> &u_nsplit, std::vector<long long> &u_part) {
   const beam_geom &g = p->geom;
   DevPlan &d = p->d;
   auto floorA = [A](int v) { return v - (((v % A) + A) % A); };
@@ -234,6 +236,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   }
   // tiles and groups
   for (int u = 0; u < d.n_used; ++u) {
+    if (!own[u]) continue;
     int cf = u_cfirst[u], nc = u_ncombo[u];
     int p3min = 1 << 30;
     for (int c = cf; c < cf + nc; ++c) p3min = std::min(p3min, -combo_p1[c] - combo_p2[c]);
@@ -288,6 +291,10 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   u_nsplit.assign(d.n_used, 1);
   u_part.assign(d.n_used + 1, 0);
   for (int u = 0; u < d.n_used; ++u) {
+    if (!own[u]) {
+      u_part[u + 1] = u_part[u] + u_ncombo[u];
+      continue;
+    }
     const long long nt = p->tri_first[u + 1] - p->tri_first[u];
     std::vector<int2> runs;  // (length, k2)
     for (long long k = k2base[u]; k < k2base[u + 1]; ++k)
@@ -363,12 +370,21 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
       }
     }
   }
-  // consistency: every combo in exactly one tile slot, every triangle in exactly one chunk
+  // consistency: every owned combo in exactly one tile slot, every owned
+  // triangle in exactly one chunk
   {
     std::vector<char> seen(combo_p1.size(), 0);
+    long long owned_terms = 0;
+    for (int u = 0; u < d.n_used; ++u) {
+      if (own[u]) {
+        owned_terms += p->tri_first[u + 1] - p->tri_first[u];
+        continue;
+      }
+      for (int c = u_cfirst[u]; c < u_cfirst[u] + u_ncombo[u]; ++c) seen[c] = 2;
+    }
     for (int32_t c : tile_combo)
       if (c >= 0) {
-        if (seen[c]) return set_detail("combo placed twice"), BEAM_EINVAL;
+        if (seen[c]) return set_detail("combo placed twice or outside its shard"), BEAM_EINVAL;
         seen[c] = 1;
       }
     for (char v : seen)
@@ -384,7 +400,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
       }
       if (lsum != nt) return set_detail("chunk length"), BEAM_EINVAL;
     }
-    if (covered != d.n_terms || piece_sum != d.n_terms) return set_detail("chunks do not cover the triangle lists"), BEAM_EINVAL;
+    if (covered != owned_terms || piece_sum != owned_terms)
+      return set_detail("chunks do not cover the triangle lists"), BEAM_EINVAL;
   }
   // grouped by tile count (one launch per count, CTAs of that many warps),
   // largest work first within a group so each launch ends on small items
@@ -544,10 +561,22 @@ int build_plan_tables(beam_gpu_plan *p) {
     ep_cnt[i] = (int32_t)(p->tri_first[u + 1] - p->tri_first[u]);
   }
 
+  // ring triplets this shard sums: longest-processing-time assignment by
+  // work = accepted triangles x in-plane triangles
+  std::vector<char> own(d.n_used, 1);
+  p->u_owner.assign(d.n_used, 0);
+  if (p->cfg.shard_count > 1) {
+    std::vector<double> uwork(d.n_used);
+    for (int u = 0; u < d.n_used; ++u)
+      uwork[u] = (double)u_ncombo[u] * (double)(p->tri_first[u + 1] - p->tri_first[u]);
+    beam_shard_assign(uwork.data(), d.n_used, p->cfg.shard_count, p->u_owner.data());
+    for (int u = 0; u < d.n_used; ++u) own[u] = (p->u_owner[u] == p->cfg.shard_index);
+  }
+
   // work decomposition of the triangle-sum kernel
   std::vector<int32_t> u_nsplit;
   std::vector<long long> u_part;
-  BEAM_TRY(build_work(p, u_cfirst, u_ncombo, combo_p1, combo_p2, k2cnt, A, u_nsplit, u_part));
+  BEAM_TRY(build_work(p, u_cfirst, u_ncombo, combo_p1, combo_p2, k2cnt, own, A, u_nsplit, u_part));
   d.n_part = u_part[d.n_used];
   u_part.pop_back();
   u_cfirst.pop_back();
@@ -563,38 +592,17 @@ int build_plan_tables(beam_gpu_plan *p) {
   BEAM_TRY(upload(p, &d.ep_pz, ep_pz));
   BEAM_TRY(upload(p, &d.ep_cnt, ep_cnt));
 
-  // per-realization buffers
-  BEAM_TRY(dev_alloc(p, &d.staging, (size_t)d.n_modes * Q * 2));
-  if (p->cfg.precision == BEAM_PREC_MIXED)
-    BEAM_TRY(dev_alloc(p, &d.S32, (size_t)d.n_modes * d.W * 2));
-  else
-    BEAM_TRY(dev_alloc(p, &d.S64, (size_t)d.n_modes * d.W * 2));
-  BEAM_TRY(dev_alloc(p, &d.part, (size_t)d.n_part));
-  BEAM_TRY(dev_alloc(p, &d.B, (size_t)ntri));
-  BEAM_TRY(dev_alloc(p, &d.bins, (size_t)3 * d.n_bins * BEAM_NPOLES));
-  BEAM_TRY(dev_alloc(p, &d.bin_count, (size_t)d.n_bins));
-  BEAM_TRY(dev_alloc(p, &d.status, 1));
-  BEAM_CUDA(cudaMemset(d.status, 0, sizeof(int)));
-  BEAM_CUDA(cudaMallocHost(&p->h_staging, sizeof(double) * 2 * std::max<size_t>(1, (size_t)d.n_modes * Q)));
-  BEAM_CUDA(cudaMallocHost(&p->h_bins, sizeof(double) * 3 * std::max(1, d.n_bins) * BEAM_NPOLES));
-  BEAM_CUDA(cudaMallocHost(&p->h_count, sizeof(long long) * std::max(1, d.n_bins)));
+  d.elem = (p->cfg.precision == BEAM_PREC_MIXED) ? sizeof(float2) : sizeof(double2);
   return BEAM_OK;
 }
 
 void free_plan_tables(beam_gpu_plan *p) {
   DevPlan &d = p->d;
-  void *ptrs[] = {d.mode_ij, d.mode_neg, d.ringmap, d.pixlocal, d.tri_list, d.combo_u, d.combo_out, d.u_cfirst,
-                  d.u_ncombo, d.u_nsplit, d.u_part, d.tiles, d.tile_combo, d.chunks, d.pieces, d.descs, d.items, d.part,
-                  d.staging, d.S64, d.S32, d.B, d.bin_first, d.ep_px, d.ep_pz, d.ep_cnt, d.bins, d.bin_count,
-                  d.status};
+  void *ptrs[] = {d.mode_ij,  d.mode_neg, d.ringmap, d.pixlocal,   d.tri_list, d.combo_u, d.combo_out,
+                  d.u_cfirst, d.u_ncombo, d.u_nsplit, d.u_part,    d.tiles,    d.tile_combo, d.chunks,
+                  d.pieces,   d.descs,    d.items,    d.bin_first, d.ep_px,    d.ep_pz,   d.ep_cnt};
   for (void *q : ptrs)
     if (q) cudaFree(q);
-  if (p->h_staging) cudaFreeHost(p->h_staging);
-  if (p->h_bins) cudaFreeHost(p->h_bins);
-  if (p->h_count) cudaFreeHost(p->h_count);
-  p->h_staging = nullptr;
-  p->h_bins = nullptr;
-  p->h_count = nullptr;
   d = DevPlan();
 }
 

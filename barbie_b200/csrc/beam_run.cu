@@ -5,7 +5,9 @@
 //                  for negative planes)                          (funcs.c:94-106)
 //   k_epilogue     cal_coeff weights, bins, normalisation        (barbie.c:343-363,
 //                                                               383-392; funcs.c:708-745)
+#include <algorithm>
 #include <cstring>
+#include <new>
 
 #include "beam_device.cuh"
 #include "beam_internal.h"
@@ -28,13 +30,17 @@ struct CplxOf<float2> {
 // for q >= 0 (zero for k_perp = 0 on plane 0, funcs.c:102-106) and
 // conj(Delta(-k_m, -q)) for q < 0, the conjugate plane the reference reads with
 // sign_2/sign_3 = -1 (barbie.c:332); other columns are zero.
-// src: staged rows [n_modes][Q] (staged = 1) or the full r2c buffer.
+// srcs[r] for realization r = blockIdx.y: its staged rows [n_modes][Q]
+// (staged = 1) or its full r2c buffer; S rows of realization r start at
+// r * n_modes * W.
 template <typename C>
-__global__ void k_build_modes(const double2 *__restrict__ src, int staged, const int16_t *__restrict__ mode_ij,
+__global__ void k_build_modes(const double *const *__restrict__ srcs, int staged, const int16_t *__restrict__ mode_ij,
                               const int32_t *__restrict__ mode_neg, int n_modes, int Q, int W, int colbase, int NN,
                               C *__restrict__ S) {
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)n_modes * W) return;
+  const double2 *src = reinterpret_cast<const double2 *>(srcs[blockIdx.y]);
+  S += (size_t)blockIdx.y * n_modes * W;
   int m = (int)(idx / W), w = (int)(idx % W);
   int q = w - colbase;
   C v = CplxOf<C>::make(0.0, 0.0);
@@ -103,11 +109,12 @@ __device__ __forceinline__ void orientation_weights(double px, double pz, double
 
 constexpr int EP_THREADS = 128;
 
-// One CTA per (k1, t, mu) bin over its triangles (bin order = loop order within
-// the bin). B == 0 drops the triangle's count (barbie.c:355-357). Reduction
-// order is fixed, so results are run-to-run identical.
+// One CTA per (k1, t, mu) bin (blockIdx.x) and realization (blockIdx.y) over
+// the bin's triangles (bin order = loop order within the bin). B == 0 drops the
+// triangle's count (barbie.c:355-357). Reduction order is fixed, so results are
+// run-to-run identical and do not depend on the batch a realization runs in.
 __global__ void __launch_bounds__(EP_THREADS) k_epilogue(const int32_t *__restrict__ bin_first,
-                                                         const double *__restrict__ B,
+                                                         const double *__restrict__ B, long long b_stride,
                                                          const double *__restrict__ px,
                                                          const double *__restrict__ pz,
                                                          const int32_t *__restrict__ cnt, double nn2, double vol,
@@ -116,6 +123,9 @@ __global__ void __launch_bounds__(EP_THREADS) k_epilogue(const int32_t *__restri
   __shared__ double red[2 * BEAM_NPOLES][EP_THREADS];
   __shared__ long long redc[EP_THREADS];
   const int b = blockIdx.x, tid = threadIdx.x;
+  B += (size_t)blockIdx.y * b_stride;
+  bins += (size_t)blockIdx.y * 3 * n_bins * BEAM_NPOLES;
+  bin_count += (size_t)blockIdx.y * n_bins;
   double sb[BEAM_NPOLES], sn[BEAM_NPOLES];
 #pragma unroll
   for (int k = 0; k < BEAM_NPOLES; ++k) sb[k] = sn[k] = 0.0;
@@ -158,72 +168,267 @@ __global__ void __launch_bounds__(EP_THREADS) k_epilogue(const int32_t *__restri
 }
 
 // ------------------------------------------------------------ host drivers
-int upload_modes_host(beam_gpu_plan *p, const double *r2c) {
-  DevPlan &d = p->d;
-  const long NN = p->geom.NN, NH = NN / 2 + 1;
-  const int Q = d.Q;
-  for (int m = 0; m < d.n_modes; ++m) {
-    size_t row = ((size_t)p->mode_ij[2 * m] * NN + (size_t)p->mode_ij[2 * m + 1]) * (size_t)NH;
-    std::memcpy(p->h_staging + (size_t)2 * m * Q, r2c + 2 * row, sizeof(double) * 2 * Q);
+int lane_create(Lane *l) {
+  cudaError_t e = cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking);
+  for (int k = 0; k < TRI_WARPS && e == cudaSuccess; ++k) {
+    e = cudaStreamCreateWithFlags(&l->side[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l->join[k], cudaEventDisableTiming);
   }
-  cudaStream_t s = p->ctx->stream;
-  BEAM_CUDA(cudaMemcpyAsync(d.staging, p->h_staging, sizeof(double) * 2 * (size_t)d.n_modes * Q,
-                            cudaMemcpyHostToDevice, s));
-  long long n = (long long)d.n_modes * d.W;
-  if (n == 0) return BEAM_OK;
-  int blocks = (int)((n + 255) / 256);
-  if (d.S64)
-    k_build_modes<double2><<<blocks, 256, 0, s>>>((const double2 *)d.staging, 1, d.mode_ij, d.mode_neg, d.n_modes,
-                                                   Q, d.W, d.colbase, (int)NN, (double2 *)d.S64);
-  else
-    k_build_modes<float2><<<blocks, 256, 0, s>>>((const double2 *)d.staging, 1, d.mode_ij, d.mode_neg, d.n_modes, Q,
-                                                  d.W, d.colbase, (int)NN, (float2 *)d.S32);
-  BEAM_CUDA(cudaGetLastError());
-  return BEAM_OK;
-}
-
-int upload_modes_device(beam_gpu_plan *p, const double *r2c_dev) {
-  DevPlan &d = p->d;
-  cudaStream_t s = p->ctx->stream;
-  long long n = (long long)d.n_modes * d.W;
-  if (n == 0) return BEAM_OK;
-  int blocks = (int)((n + 255) / 256);
-  if (d.S64)
-    k_build_modes<double2><<<blocks, 256, 0, s>>>((const double2 *)r2c_dev, 0, d.mode_ij, d.mode_neg, d.n_modes, d.Q,
-                                                   d.W, d.colbase, (int)p->geom.NN, (double2 *)d.S64);
-  else
-    k_build_modes<float2><<<blocks, 256, 0, s>>>((const double2 *)r2c_dev, 0, d.mode_ij, d.mode_neg, d.n_modes, d.Q,
-                                                  d.W, d.colbase, (int)p->geom.NN, (float2 *)d.S32);
-  BEAM_CUDA(cudaGetLastError());
-  return BEAM_OK;
-}
-
-int run_epilogue(beam_gpu_plan *p) {
-  DevPlan &d = p->d;
-  cudaStream_t s = p->ctx->stream;
-  if (d.n_bins == 0) return BEAM_OK;
-  double nn2 = (double)p->geom.NN * (double)p->geom.NN;
-  k_epilogue<<<d.n_bins, EP_THREADS, 0, s>>>(d.bin_first, d.B, d.ep_px, d.ep_pz, d.ep_cnt, nn2, p->geom.vol,
-                                             d.n_bins, d.bins, d.bin_count);
-  BEAM_CUDA(cudaGetLastError());
-  return BEAM_OK;
-}
-
-int check_status(beam_gpu_plan *p) {
-  int st = 0;
-  BEAM_CUDA(cudaMemcpyAsync(&st, p->d.status, sizeof(int), cudaMemcpyDeviceToHost, p->ctx->stream));
-  BEAM_CUDA(cudaStreamSynchronize(p->ctx->stream));
-  if (st & DEV_TIMEOUT) {
-    set_detail("a bounded device wait in the triangle-sum kernel gave up");
-    cudaMemsetAsync(p->d.status, 0, sizeof(int), p->ctx->stream);
-    return BEAM_ETIMEDOUT;
-  }
-  if (st) {
-    set_detail("device reported a bad index");
-    cudaMemsetAsync(p->d.status, 0, sizeof(int), p->ctx->stream);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    set_detail(std::string("stream/event creation: ") + cudaGetErrorString(e));
+    lane_destroy(l);
     return BEAM_ECUDA;
   }
   return BEAM_OK;
 }
 
+void lane_destroy(Lane *l) {
+  for (int k = 0; k < TRI_WARPS; ++k) {
+    if (l->side[k]) cudaStreamDestroy(l->side[k]);
+    if (l->join[k]) cudaEventDestroy(l->join[k]);
+  }
+  if (l->fork) cudaEventDestroy(l->fork);
+  if (l->stream) cudaStreamDestroy(l->stream);
+  *l = Lane();
+}
+
+// Sizes of a slot's device buffers, in the order slot_alloc allocates them.
+struct SlotSizes {
+  size_t staging, src, S, part, B, bins, count;
+};
+static SlotSizes slot_sizes(const beam_gpu_plan *p, int cap) {
+  const DevPlan &d = p->d;
+  const size_t c = (size_t)cap;
+  SlotSizes z;
+  z.staging = sizeof(double) * 2 * c * (size_t)d.n_modes * d.Q;
+  z.src = sizeof(double *) * 2 * c;
+  z.S = d.elem * c * (size_t)d.n_modes * d.W;
+  z.part = sizeof(double) * c * (size_t)d.n_part;
+  z.B = sizeof(double) * c * (size_t)std::max<long long>(1, d.n_combo);
+  z.bins = sizeof(double) * c * 3 * (size_t)d.n_bins * BEAM_NPOLES;
+  z.count = sizeof(long long) * c * (size_t)d.n_bins;
+  return z;
+}
+
+size_t slot_bytes(const beam_gpu_plan *p, int cap) {
+  SlotSizes z = slot_sizes(p, cap);
+  return z.staging + z.src + z.S + z.part + z.B + z.bins + z.count + sizeof(int);
+}
+
+void slot_destroy(RunSlot *s) {
+  if (!s) return;
+  if (s->lane && s->lane->stream) cudaStreamSynchronize(s->lane->stream);
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  void *dev[] = {s->staging, (void *)s->src, s->S, s->part, s->B, s->bins, s->bin_count, s->status};
+  for (void *q : dev)
+    if (q) cudaFree(q);
+  void *host[] = {s->h_staging, (void *)s->h_src, s->h_bins, s->h_count, s->h_status};
+  for (void *q : host)
+    if (q) cudaFreeHost(q);
+  for (int k = 0; k < 5; ++k)
+    if (s->ev[k]) cudaEventDestroy(s->ev[k]);
+  if (s->done) cudaEventDestroy(s->done);
+  lane_destroy(&s->own);
+  delete s;
+}
+
+static int slot_alloc(beam_gpu_plan *p, RunSlot *s) {
+  const DevPlan &d = p->d;
+  const int cap = s->cap;
+  SlotSizes z = slot_sizes(p, cap);
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->staging, z.staging));
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->src, z.src));
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->S, z.S));
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->part, z.part));
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->B, z.B));
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->bins, z.bins));
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->bin_count, z.count));
+  BEAM_TRY(dev_alloc(&s->bytes, &s->status, 1));
+  BEAM_CUDA(cudaMallocHost(&s->h_staging, std::max<size_t>(16, z.staging)));
+  BEAM_CUDA(cudaMallocHost((void **)&s->h_src, z.src));
+  BEAM_CUDA(cudaMallocHost(&s->h_bins, std::max<size_t>(16, z.bins)));
+  BEAM_CUDA(cudaMallocHost(&s->h_count, std::max<size_t>(16, z.count)));
+  BEAM_CUDA(cudaMallocHost(&s->h_status, sizeof(int)));
+  *s->h_status = 0;
+  for (int k = 0; k < 5; ++k) BEAM_CUDA(cudaEventCreate(&s->ev[k]));
+  BEAM_CUDA(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
+  // staged sources are fixed: realization r reads staging rows r
+  for (int r = 0; r < cap; ++r) {
+    s->h_src[r] = s->staging + (size_t)2 * r * d.n_modes * d.Q;
+    s->h_src[cap + r] = nullptr;
+  }
+  cudaStream_t st = s->lane->stream;
+  BEAM_CUDA(cudaMemcpyAsync((void *)s->src, s->h_src, z.src, cudaMemcpyHostToDevice, st));
+  // partial sums that no CTA writes (ring triplets of other shards) stay zero
+  BEAM_CUDA(cudaMemsetAsync(s->part, 0, z.part, st));
+  BEAM_CUDA(cudaMemsetAsync(s->status, 0, sizeof(int), st));
+  BEAM_CUDA(cudaStreamSynchronize(st));
+  return BEAM_OK;
+}
+
+int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out) {
+  *out = nullptr;
+  if (cap < 1 || cap > 65535) {
+    set_detail("slot capacity must be 1..65535 realizations");
+    return BEAM_EINVAL;
+  }
+  RunSlot *s = new (std::nothrow) RunSlot();
+  if (!s) return BEAM_ENOMEM;
+  s->cap = cap;
+  int rc = BEAM_OK;
+  if (lane) {
+    s->lane = lane;
+  } else {
+    rc = lane_create(&s->own);
+    s->lane = &s->own;
+  }
+  if (rc == BEAM_OK) rc = slot_alloc(p, s);
+  if (rc != BEAM_OK) {
+    slot_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return BEAM_OK;
+}
+
+// Copy the plan's mode rows of one host r2c buffer into the slot's pinned
+// staging rows of realization r (funcs.c:94-106 reads the same elements).
+void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c) {
+  const DevPlan &d = p->d;
+  const long NN = p->geom.NN, NH = NN / 2 + 1;
+  const int Q = d.Q;
+  double *dst = s->h_staging + (size_t)2 * r * d.n_modes * Q;
+  for (int m = 0; m < d.n_modes; ++m) {
+    size_t row = ((size_t)p->mode_ij[2 * m] * NN + (size_t)p->mode_ij[2 * m + 1]) * (size_t)NH;
+    std::memcpy(dst + (size_t)2 * m * Q, r2c + 2 * row, sizeof(double) * 2 * Q);
+  }
+}
+
+// Mode rows of realizations [0, n): from the pinned staging rows (staged) or
+// from the device r2c buffers the caller put in h_src[cap + r].
+int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged) {
+  const DevPlan &d = p->d;
+  cudaStream_t st = s->lane->stream;
+  if (staged) {
+    BEAM_CUDA(cudaMemcpyAsync(s->staging, s->h_staging, sizeof(double) * 2 * (size_t)n * d.n_modes * d.Q,
+                              cudaMemcpyHostToDevice, st));
+  } else {
+    BEAM_CUDA(cudaMemcpyAsync((void *)(s->src + s->cap), s->h_src + s->cap, sizeof(double *) * n,
+                              cudaMemcpyHostToDevice, st));
+  }
+  long long per = (long long)d.n_modes * d.W;
+  if (per == 0) return BEAM_OK;
+  dim3 grid((unsigned)((per + 255) / 256), (unsigned)n);
+  const double *const *srcs = staged ? s->src : s->src + s->cap;
+  if (d.elem == sizeof(double2))
+    k_build_modes<double2><<<grid, 256, 0, st>>>(srcs, staged ? 1 : 0, d.mode_ij, d.mode_neg, d.n_modes, d.Q, d.W,
+                                                 d.colbase, (int)p->geom.NN, (double2 *)s->S);
+  else
+    k_build_modes<float2><<<grid, 256, 0, st>>>(srcs, staged ? 1 : 0, d.mode_ij, d.mode_neg, d.n_modes, d.Q, d.W,
+                                                d.colbase, (int)p->geom.NN, (float2 *)s->S);
+  BEAM_CUDA(cudaGetLastError());
+  s->launches++;
+  return BEAM_OK;
+}
+
+int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n) {
+  const DevPlan &d = p->d;
+  if (d.n_bins == 0) return BEAM_OK;
+  double nn2 = (double)p->geom.NN * (double)p->geom.NN;
+  long long b_stride = std::max<long long>(1, d.n_combo);
+  k_epilogue<<<dim3((unsigned)d.n_bins, (unsigned)n), EP_THREADS, 0, s->lane->stream>>>(
+      d.bin_first, s->B, b_stride, d.ep_px, d.ep_pz, d.ep_cnt, nn2, p->geom.vol, d.n_bins, s->bins, s->bin_count);
+  BEAM_CUDA(cudaGetLastError());
+  s->launches++;
+  return BEAM_OK;
+}
+
+// Queue the copies of realizations [0, n)'s bins, counts and the status word
+// to the slot's pinned host buffers, then the slot's `done` event.
+int fetch_results(beam_gpu_plan *p, RunSlot *s, int n) {
+  const DevPlan &d = p->d;
+  cudaStream_t st = s->lane->stream;
+  size_t nb = (size_t)d.n_bins;
+  if (nb) {
+    BEAM_CUDA(cudaMemcpyAsync(s->h_bins, s->bins, sizeof(double) * n * 3 * nb * BEAM_NPOLES, cudaMemcpyDeviceToHost,
+                              st));
+    BEAM_CUDA(cudaMemcpyAsync(s->h_count, s->bin_count, sizeof(long long) * n * nb, cudaMemcpyDeviceToHost, st));
+  }
+  BEAM_CUDA(cudaMemcpyAsync(s->h_status, s->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BEAM_CUDA(cudaEventRecord(s->done, st));
+  return BEAM_OK;
+}
+
+// Wait for the slot's last queued run and turn the device status word into an
+// error code (clearing it for the next run).
+int check_status(RunSlot *s) {
+  BEAM_CUDA(cudaEventSynchronize(s->done));
+  int st = *s->h_status;
+  if (st == 0) return BEAM_OK;
+  *s->h_status = 0;
+  cudaMemsetAsync(s->status, 0, sizeof(int), s->lane->stream);
+  if (st & DEV_TIMEOUT) {
+    set_detail("a bounded device wait in the triangle-sum kernel gave up");
+    return BEAM_ETIMEDOUT;
+  }
+  set_detail("device reported a bad index");
+  return BEAM_ECUDA;
+}
+
+// Bins of realization r from the slot's pinned copies (after check_status).
+int copy_result(const beam_gpu_plan *p, const RunSlot *s, int r, beam_result *res) {
+  if (!res) return BEAM_OK;
+  size_t nb = (size_t)p->d.n_bins, n = nb * BEAM_NPOLES;
+  const double *h = s->h_bins + (size_t)r * 3 * n;
+  if (res->bs) std::memcpy(res->bs, h, sizeof(double) * n);
+  if (res->norm) std::memcpy(res->norm, h + n, sizeof(double) * n);
+  if (res->out) std::memcpy(res->out, h + 2 * n, sizeof(double) * n);
+  if (res->count)
+    for (size_t b = 0; b < nb; ++b) res->count[b] = (int64_t)s->h_count[(size_t)r * nb + b];
+  return BEAM_OK;
+}
+
+// One host-input run of realizations [0, n) whose staging rows are gathered:
+// H2D of the rows, mode build, triangle sums, epilogue and D2H of the bins,
+// captured once per n into a CUDA graph and replayed.
+int slot_run_graph(beam_gpu_plan *p, RunSlot *s, int n) {
+  cudaStream_t st = s->lane->stream;
+  if (!s->graph || s->graph_n != n) {
+    if (s->graph) cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    s->graph_n = 0;
+    BEAM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    s->launches = 0;
+    s->capturing = true;
+    int rc = upload_modes(p, s, n, true);
+    if (rc == BEAM_OK) rc = run_triangle_sums(p, s, n);
+    if (rc == BEAM_OK) rc = run_epilogue(p, s, n);
+    if (rc == BEAM_OK) rc = fetch_results(p, s, n);
+    s->capturing = false;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != BEAM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) {
+      set_detail(std::string("graph capture: ") + cudaGetErrorString(e));
+      return BEAM_ECUDA;
+    }
+    e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      s->graph = nullptr;
+      set_detail(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      return BEAM_ECUDA;
+    }
+    s->graph_n = n;
+  }
+  s->timed = false;
+  BEAM_CUDA(cudaGraphLaunch(s->graph, st));
+  // the graph ends with fetch_results; `done` must follow this replay
+  BEAM_CUDA(cudaEventRecord(s->done, st));
+  return BEAM_OK;
+}
 }  // namespace beam

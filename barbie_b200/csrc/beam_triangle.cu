@@ -45,7 +45,10 @@ struct TriArgs {
   const long long *u_part;
   double *part;
   int *status;
-  int stage;  // complex values per stage
+  int stage;              // complex values per stage
+  int nreal;              // realizations per launch (blockIdx.y)
+  long long s_stride;     // complex values of S per realization
+  long long part_stride;  // partial sums per realization
 };
 
 // What the producer needs to issue one chunk's copies, loaded one chunk ahead
@@ -91,7 +94,7 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[TRI_STAGES], empty[TRI_STAGES];
   __shared__ volatile int s_fail;
-  const TriItem it = a.items[blockIdx.x];
+  const TriItem it = a.items[blockIdx.x];  // realization blockIdx.y
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ncons = (blockDim.x >> 5) - 1;  // consumer warps == it.ntiles; warp ncons produces
   if (tid == 0) {
@@ -104,7 +107,7 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
   }
   __syncthreads();
   C *stages = reinterpret_cast<C *>(smem_raw);
-  const C *S = static_cast<const C *>(a.S);
+  const C *S = static_cast<const C *>(a.S) + (size_t)blockIdx.y * a.s_stride;
   const int nch = it.ch1 - it.ch0;
 
   if (warp == ncons) {
@@ -197,7 +200,8 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
     if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
   }
   const int nc = a.u_ncombo[it.u];
-  double *out = a.part + a.u_part[it.u] + (long long)it.split * nc - a.u_cfirst[it.u];
+  double *out = a.part + (long long)blockIdx.y * a.part_stride + a.u_part[it.u] + (long long)it.split * nc -
+                a.u_cfirst[it.u];
 #pragma unroll
   for (int q = 0; q < TRI_P1; ++q) {
     const int cidx = tc[q * 32];
@@ -206,13 +210,16 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
 }
 
 // Sum the splits of each combo in split order, scale by NN^2 and store the
-// triangle's B at its bin-order position.
+// triangle's B at its bin-order position; realization blockIdx.y.
 __global__ void k_reduce(long long n_combo, const int32_t *__restrict__ combo_u, const int32_t *__restrict__ u_cfirst,
                          const int32_t *__restrict__ u_ncombo, const int32_t *__restrict__ u_nsplit,
                          const long long *__restrict__ u_part, const int32_t *__restrict__ combo_out,
-                         const double *__restrict__ part, double nn2, double *__restrict__ B) {
+                         const double *__restrict__ part, long long part_stride, double nn2,
+                         double *__restrict__ B, long long b_stride) {
   long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_combo) return;
+  part += (long long)blockIdx.y * part_stride;
+  B += (long long)blockIdx.y * b_stride;
   int u = combo_u[c];
   int nc = u_ncombo[u], ns = u_nsplit[u];
   const double *p = part + u_part[u] + (c - u_cfirst[u]);
@@ -227,38 +234,54 @@ static size_t tri_smem(int stage, int ntiles) {
   return (size_t)TRI_STAGES * stage * sizeof(C);
 }
 
-// One launch per tile count n (CTAs of n consumer warps + 1 producer warp), on
-// side streams forked from and joined back into the context's stream, so the
-// launches overlap.
+// Allow both instantiations the device's opt-in shared memory (less their
+// static barriers) once per context; each launch still asks only for its
+// class's stages.
 template <typename C>
-static int launch_classes(beam_gpu_plan *p, TriArgs a) {
+static int allow_optin(size_t smem_optin) {
+  cudaFuncAttributes fa;
+  BEAM_CUDA(cudaFuncGetAttributes(&fa, k_triangle<C>));
+  int dyn = (int)(smem_optin > fa.sharedSizeBytes ? smem_optin - fa.sharedSizeBytes : 0);
+  BEAM_CUDA(cudaFuncSetAttribute(k_triangle<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+  return BEAM_OK;
+}
+
+int triangle_init_attributes(size_t smem_optin) {
+  BEAM_TRY(allow_optin<double2>(smem_optin));
+  BEAM_TRY(allow_optin<float2>(smem_optin));
+  return BEAM_OK;
+}
+
+// One launch per tile count n (CTAs of n consumer warps + 1 producer warp), on
+// side streams forked from and joined back into the slot's stream, so the
+// launches overlap. Each launch covers its class's items for all realizations
+// (blockIdx.y).
+template <typename C>
+static int launch_classes(beam_gpu_plan *p, RunSlot *s, TriArgs a) {
   DevPlan &d = p->d;
-  beam_gpu_ctx *ctx = p->ctx;
-  size_t max_smem = 0;
-  for (int n = 1; n <= TRI_WARPS; ++n) max_smem = std::max(max_smem, tri_smem<C>(d.class_stage[n], n));
-  BEAM_CUDA(cudaFuncSetAttribute(k_triangle<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
-  BEAM_CUDA(cudaEventRecord(ctx->fork, ctx->stream));
+  Lane *ln = s->lane;
+  BEAM_CUDA(cudaEventRecord(ln->fork, ln->stream));
   for (int n = TRI_WARPS; n >= 1; --n) {
     int first = d.class_first[n], count = d.class_first[n + 1] - first;
     if (count == 0) continue;
-    cudaStream_t st = ctx->side[n - 1];
-    BEAM_CUDA(cudaStreamWaitEvent(st, ctx->fork, 0));
+    cudaStream_t st = ln->side[n - 1];
+    BEAM_CUDA(cudaStreamWaitEvent(st, ln->fork, 0));
     TriArgs b = a;
     b.items = d.items + first;
     b.stage = d.class_stage[n];
-    k_triangle<C><<<count, 32 * (n + 1), tri_smem<C>(b.stage, n), st>>>(b);
+    k_triangle<C><<<dim3((unsigned)count, (unsigned)a.nreal), 32 * (n + 1), tri_smem<C>(b.stage, n), st>>>(b);
     BEAM_CUDA(cudaGetLastError());
-    BEAM_CUDA(cudaEventRecord(ctx->join[n - 1], st));
-    BEAM_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->join[n - 1], 0));
+    s->launches++;
+    BEAM_CUDA(cudaEventRecord(ln->join[n - 1], st));
+    BEAM_CUDA(cudaStreamWaitEvent(ln->stream, ln->join[n - 1], 0));
   }
   return BEAM_OK;
 }
 
-int run_triangle_sums(beam_gpu_plan *p) {
+int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n) {
   DevPlan &d = p->d;
-  cudaStream_t s = p->ctx->stream;
   if (d.n_combo == 0) {
-    for (int k = 1; k <= 3; ++k) mark(p, k);
+    for (int k = 1; k <= 3; ++k) mark(s, k);
     return BEAM_OK;
   }
   TriArgs a;
@@ -266,28 +289,31 @@ int run_triangle_sums(beam_gpu_plan *p) {
   a.tiles = d.tiles;
   a.tile_combo = d.tile_combo;
   a.descs = d.descs;
+  a.S = s->S;
   a.W = d.W;
   a.colbase = d.colbase;
   a.u_cfirst = d.u_cfirst;
   a.u_ncombo = d.u_ncombo;
   a.u_part = d.u_part;
-  a.part = d.part;
-  a.status = d.status;
+  a.part = s->part;
+  a.status = s->status;
   a.stage = 0;
-  mark(p, 1);
-  if (d.S64) {
-    a.S = d.S64;
-    BEAM_TRY(launch_classes<double2>(p, a));
-  } else {
-    a.S = d.S32;
-    BEAM_TRY(launch_classes<float2>(p, a));
-  }
-  mark(p, 2);
+  a.nreal = n;
+  a.s_stride = (long long)d.n_modes * d.W;
+  a.part_stride = d.n_part;
+  mark(s, 1);
+  if (d.elem == sizeof(double2))
+    BEAM_TRY(launch_classes<double2>(p, s, a));
+  else
+    BEAM_TRY(launch_classes<float2>(p, s, a));
+  mark(s, 2);
   double nn2 = (double)p->geom.NN * (double)p->geom.NN;
-  k_reduce<<<(unsigned)((d.n_combo + 255) / 256), 256, 0, s>>>(d.n_combo, d.combo_u, d.u_cfirst, d.u_ncombo,
-                                                               d.u_nsplit, d.u_part, d.combo_out, d.part, nn2, d.B);
+  dim3 grid((unsigned)((d.n_combo + 255) / 256), (unsigned)n);
+  k_reduce<<<grid, 256, 0, s->lane->stream>>>(d.n_combo, d.combo_u, d.u_cfirst, d.u_ncombo, d.u_nsplit, d.u_part,
+                                              d.combo_out, s->part, d.n_part, nn2, s->B, d.n_combo);
   BEAM_CUDA(cudaGetLastError());
-  mark(p, 3);
+  s->launches++;
+  mark(s, 3);
   return BEAM_OK;
 }
 

@@ -274,7 +274,10 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(fields[0], info)
 
-    gpu_launches = 4 * args.steps  # build_modes, triangle, reduce, epilogue per step
+    # kernels per bispectrum as the library counted them in the last run: mode
+    # build, one triangle-sum launch per tile class, split reduction, epilogue
+    per_run = plan.refresh_info()["launches_last_run"]
+    gpu_launches = per_run * args.steps
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

@@ -73,10 +73,26 @@ typedef struct beam_cfg {
   double LL;      /* cell size for vol=(NN*LL)^3 (barbie.c:67,76) */
   int precision;  /* BEAM_PREC_* */
   int method;     /* BEAM_METHOD_* */
+  /* One bispectrum split over several GPUs (the analogue of the reference's
+   * MPI estimator splitting its loop over ranks, zBS_fast_mpi.c:149,294-296):
+   * the plan sums only the ring triplets beam_shard_assign gives shard_index
+   * of shard_count, and its bs/norm/count are partial sums that add up across
+   * the shards (out is then bs/(vol*norm) of the sums). shard_count 0 or 1:
+   * the whole estimator. Triangle method only. */
+  int shard_index;
+  int shard_count;
 } beam_cfg;
 
 /* Fill cfg with the reference's defaults for the given command-line values. */
 BEAM_API void beam_cfg_default(beam_cfg *cfg, long NN, int UL_k1, int LL_k1, int BW_k1);
+
+/* Longest-processing-time assignment of n work units (ring triplets, in
+ * increasing calCR order) to shard_count shards: units in order of decreasing
+ * work (ties: lower index first) each go to the shard with the least work so
+ * far (ties: lower shard). Host-only and deterministic, so every rank computes
+ * the same owner[] from the same work[]. No counterpart in the reference,
+ * whose MPI variants split planes round-robin. */
+BEAM_API int beam_shard_assign(const double *work, int n, int shard_count, int *owner);
 
 /* Estimator output; any pointer may be NULL. */
 typedef struct beam_result {
@@ -98,6 +114,9 @@ typedef struct beam_plan_info {
   int n_planes;           /* planes |p| in use (0..n_planes-1) */
   size_t device_bytes;    /* device memory held by the plan (tables + per-run buffers) */
   double vol;             /* (NN*LL)^3 */
+  long n_shard_terms;     /* in-plane triangles this plan's shard sums (n_fourier_terms unsharded) */
+  int launches_last_run;  /* kernels the plan's last beam_gpu_run / triangle_sums call launched */
+  size_t run_bytes;       /* device bytes of the buffers of one more concurrent realization */
 } beam_plan_info;
 
 /* Library / device setup. Replaces the fftw_init_threads / plan_with_nthreads
@@ -122,11 +141,19 @@ BEAM_API int beam_gpu_plan_get_info(const beam_gpu_plan *plan, beam_plan_info *i
  * pinned) or device memory (r2c_on_device=1). Results go to host memory. */
 BEAM_API int beam_gpu_run(beam_gpu_plan *plan, const double *r2c, int r2c_on_device, beam_result *res);
 
-/* Several realizations of one plan in one call: the per-realization mode data
- * and partial sums stay on the device and all realizations' triangle sums run
- * in one launch sequence (captured once into a CUDA graph and replayed).
- * r2c[i] are host buffers; res[i] receives realization i. */
+/* Several realizations of one plan in one call (no counterpart in the
+ * reference, which runs one realization per process). Realizations go to the
+ * device in batches: each kernel of a batch (mode build, the per-class
+ * triangle sums, split reduction, epilogue) is one launch over all of the
+ * batch's realizations, and the batch's sequence -- H2D of the gathered mode
+ * rows, kernels, D2H of the bins -- is captured once into a CUDA graph and
+ * replayed. Two batch buffers alternate, so the host gathers batch i+1 while
+ * the device runs batch i. Results equal beam_gpu_run's bit for bit.
+ * r2c[i] are host buffers; res[i] receives realization i (res may be NULL).
+ * batch: realizations per batch, 0 = chosen from free device memory (<= n). */
 BEAM_API int beam_gpu_run_batch(beam_gpu_plan *plan, const double *const *r2c, int n, beam_result *res);
+BEAM_API int beam_gpu_run_batch_ex(beam_gpu_plan *plan, const double *const *r2c, int n, beam_result *res,
+                                   int batch);
 
 /* calCR (funcs.c:328-424): closed ring triplets in the reference's order as
  * records {r1, r2, r3, Num} with Num = NN^2 * (exact triangle count) -- the
