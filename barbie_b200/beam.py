@@ -297,3 +297,115 @@ class Plan:
         NN = self.NN
         if tuple(r2c.shape) not in ((NN, NN, NN + 2), (NN * NN * (NN + 2),)):
             raise ValueError(f"r2c buffer must be [{NN}][{NN}][{NN + 2}] float64")
+
+
+class ServerCfg(ctypes.Structure):
+    _fields_ = [("mem_budget", ctypes.c_size_t), ("max_active", ctypes.c_int), ("max_plans", ctypes.c_int)]
+
+
+class JobInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("error", ctypes.c_int), ("n_k1bin", ctypes.c_int), ("n_mtbin", ctypes.c_int),
+                ("n_bins", ctypes.c_long), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
+def _server_protos(L) -> None:
+    if getattr(L, "_server_protos", False):
+        return
+    vp = ctypes.c_void_p
+    L.beam_server_cfg_default.argtypes = [ctypes.POINTER(ServerCfg)]
+    L.beam_server_cfg_default.restype = None
+    L.beam_gpu_server_create.argtypes = [vp, ctypes.POINTER(ServerCfg), ctypes.POINTER(vp)]
+    L.beam_gpu_server_destroy.argtypes = [vp]
+    L.beam_gpu_server_destroy.restype = None
+    L.beam_gpu_server_submit.argtypes = [vp, ctypes.POINTER(Cfg), vp, ctypes.POINTER(ctypes.c_int64)]
+    L.beam_gpu_server_wait.argtypes = [vp, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(JobInfo)]
+    L.beam_gpu_server_take.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(Result)]
+    L.beam_gpu_server_memory.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+    for name in ("beam_gpu_server_create", "beam_gpu_server_submit", "beam_gpu_server_wait", "beam_gpu_server_take",
+                 "beam_gpu_server_memory"):
+        getattr(L, name).restype = ctypes.c_int
+    L._server_protos = True
+
+
+class Server:
+    """Job server on a context (beam_gpu_server_*): submit realizations of any
+    configuration as they arrive; they run concurrently on the device."""
+
+    def __init__(self, ctx: Context, mem_budget: int = 0, max_active: int = 0, max_plans: int = 0):
+        L = load()
+        _server_protos(L)
+        cfg = ServerCfg()
+        L.beam_server_cfg_default(ctypes.byref(cfg))
+        if mem_budget:
+            cfg.mem_budget = mem_budget
+        if max_active:
+            cfg.max_active = max_active
+        if max_plans:
+            cfg.max_plans = max_plans
+        h = ctypes.c_void_p()
+        _check(L.beam_gpu_server_create(ctx._h, ctypes.byref(cfg), ctypes.byref(h)), "beam_gpu_server_create")
+        self._h, self.ctx = h, ctx
+        self._held = {}  # job -> r2c buffer, kept alive until the job is taken
+        ctx._plans.add(self)  # closed with the context, like plans
+
+    def submit(self, r2c, NN: int, UL_k1: int, LL_k1: int, BW_k1: int, *, Nmax: int = 100, Nr: int = 40,
+               n_mtbin: int = 5, LL: float = 1.0, precision: str = "fp64") -> int:
+        addr, dev = _ptr(r2c)
+        if dev:
+            raise TypeError("server jobs take host arrays")
+        if tuple(r2c.shape) not in ((NN, NN, NN + 2), (NN * NN * (NN + 2),)):
+            raise ValueError(f"r2c buffer must be [{NN}][{NN}][{NN + 2}] float64")
+        cfg = Cfg()
+        _lib.beam_cfg_default(ctypes.byref(cfg), NN, UL_k1, LL_k1, BW_k1)
+        cfg.Nmax, cfg.Nr, cfg.n_mtbin, cfg.LL, cfg.precision = Nmax, Nr, n_mtbin, LL, PREC[precision]
+        job = ctypes.c_int64()
+        _check(_lib.beam_gpu_server_submit(self._h, ctypes.byref(cfg), addr, ctypes.byref(job)), "beam_gpu_server_submit")
+        self._held[job.value] = r2c
+        return job.value
+
+    def wait(self, job: int, timeout_ms: int = -1) -> dict | None:
+        """Job info once it has ended (None if still queued/running at the timeout)."""
+        info = JobInfo()
+        rc = _lib.beam_gpu_server_wait(self._h, job, timeout_ms, ctypes.byref(info))
+        if rc == BEAM_EBUSY:
+            return None
+        _check(rc, "beam_gpu_server_wait")
+        return {k: getattr(info, k) for k, _ in JobInfo._fields_}
+
+    def take(self, job: int) -> dict:
+        """Bins of an ended job (raises BeamError for a failed one); forgets the job."""
+        info = self.wait(job, 0)
+        if info is None:
+            raise BeamError(BEAM_EBUSY, "beam_gpu_server_take")
+        shape = (info["n_k1bin"], info["n_mtbin"], info["n_mtbin"], NPOLES)
+        bs, nm, out = (np.zeros(shape) for _ in range(3))
+        cnt = np.zeros(shape[:3], dtype=np.int64)
+        res = Result(bs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     nm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                     cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        rc = _lib.beam_gpu_server_take(self._h, job, ctypes.byref(res))
+        self._held.pop(job, None)
+        _check(rc, "beam_gpu_server_take")
+        return dict(bs=bs, norm=nm, out=out, count=cnt, info=info)
+
+    def memory(self) -> tuple[int, int]:
+        now, peak = ctypes.c_size_t(), ctypes.c_size_t()
+        _check(_lib.beam_gpu_server_memory(self._h, ctypes.byref(now), ctypes.byref(peak)), "beam_gpu_server_memory")
+        return now.value, peak.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.beam_gpu_server_destroy(self._h)
+            self._h = None
+            self._held.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

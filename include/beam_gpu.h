@@ -210,6 +210,61 @@ BEAM_API void *beam_gpu_stream(beam_gpu_ctx *ctx);
  * [2] split reduction, [3] bins epilogue. Writes min(n, 4) values. */
 BEAM_API int beam_gpu_plan_last_timings(const beam_gpu_plan *plan, float *ms, int n);
 
+/* ------------------------------------------------------------------ serving
+ * A job server on one context (no counterpart in the reference, which runs
+ * one realization per process): estimator jobs -- one realization each, any
+ * NN / rings / bins / precision -- are submitted as they arrive and run
+ * concurrently on the device. A dispatcher thread keeps a cache of plans
+ * (geometry tables) keyed by configuration, and admits queued jobs in arrival
+ * order as soon as a job slot is free and the device memory the job needs --
+ * its plan if not cached, plus one realization's run buffers
+ * (beam_plan_info.run_bytes) -- fits the budget, evicting idle cached plans
+ * when it must; a job that does not fit lets smaller later jobs go first.
+ * Each running job has its own streams and buffers, so jobs admitted while
+ * others run overlap with them on the GPU; results do not depend on what else
+ * runs (every reduction has a fixed order). While a server runs, it alone
+ * uses its context. Jobs need the triangle method and shard_count <= 1. */
+typedef struct beam_gpu_server beam_gpu_server;
+
+typedef struct beam_server_cfg {
+  size_t mem_budget; /* device bytes for cached plans and running jobs; 0 = 80% of the free memory at creation */
+  int max_active;    /* jobs on the device at once; 0 = 4 */
+  int max_plans;     /* plans kept for reuse; 0 = 16 */
+} beam_server_cfg;
+
+#define BEAM_JOB_QUEUED 0
+#define BEAM_JOB_RUNNING 1
+#define BEAM_JOB_DONE 2
+#define BEAM_JOB_FAILED 3
+
+typedef struct beam_job_info {
+  int state;        /* BEAM_JOB_* */
+  int error;        /* BEAM_* code of a failed job */
+  int n_k1bin;      /* result shape: [n_k1bin][n_mtbin][n_mtbin][16] (known once started) */
+  int n_mtbin;
+  long n_bins;
+  double queue_ms;  /* submission to start of its device work (host clock) */
+  double run_ms;    /* start of its device work to results on the host */
+  double total_ms;  /* submission to results on the host */
+} beam_job_info;
+
+BEAM_API void beam_server_cfg_default(beam_server_cfg *cfg);
+BEAM_API int beam_gpu_server_create(beam_gpu_ctx *ctx, const beam_server_cfg *cfg, beam_gpu_server **out);
+/* Waits for queued and running jobs, then frees everything the server holds. */
+BEAM_API void beam_gpu_server_destroy(beam_gpu_server *srv);
+/* Queue one realization: r2c is a host double[NN][NN][NN+2] that must stay
+ * valid and unchanged until the job is DONE or FAILED. *job receives its id. */
+BEAM_API int beam_gpu_server_submit(beam_gpu_server *srv, const beam_cfg *cfg, const double *r2c, int64_t *job);
+/* Wait up to timeout_ms (0: poll, < 0: forever) for the job to finish.
+ * BEAM_OK when it is DONE or FAILED (info->state tells which), BEAM_EBUSY
+ * when still queued or running, BEAM_ENOTFOUND for an unknown job. */
+BEAM_API int beam_gpu_server_wait(beam_gpu_server *srv, int64_t job, int timeout_ms, beam_job_info *info);
+/* Copy a DONE job's bins into res (any pointer may be NULL) and forget the
+ * job; a FAILED job returns its error and is forgotten too. */
+BEAM_API int beam_gpu_server_take(beam_gpu_server *srv, int64_t job, beam_result *res);
+/* Device bytes the server holds now (cached plans + job buffers) and at most so far. */
+BEAM_API int beam_gpu_server_memory(const beam_gpu_server *srv, size_t *now, size_t *peak);
+
 /* Human-readable text for an error code. */
 BEAM_API const char *beam_gpu_strerror(int code);
 

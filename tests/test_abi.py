@@ -61,6 +61,22 @@ def test_null_arguments_are_rejected(beamlib):
     assert L.beam_gpu_init(0, None) == beamlib.BEAM_EINVAL
     assert L.beam_gpu_plan_create(None, None, None) == beamlib.BEAM_EINVAL
     assert L.beam_gpu_run(None, None, 0, None) == beamlib.BEAM_EINVAL
+    assert L.beam_gpu_run_batch_ex(None, None, 0, None, 0) == beamlib.BEAM_EINVAL
+
+
+def test_server_host_side_argument_checks(beamlib):
+    L = beamlib.load()
+    beamlib._server_protos(L)
+    cfg = beamlib.ServerCfg()
+    L.beam_server_cfg_default(ctypes.byref(cfg))
+    assert (cfg.mem_budget, cfg.max_active, cfg.max_plans) == (0, 4, 16)
+    h = ctypes.c_void_p()
+    assert L.beam_gpu_server_create(None, ctypes.byref(cfg), ctypes.byref(h)) == beamlib.BEAM_EINVAL
+    job = ctypes.c_int64()
+    assert L.beam_gpu_server_submit(None, None, None, ctypes.byref(job)) == beamlib.BEAM_EINVAL
+    assert L.beam_gpu_server_wait(None, 1, 0, None) == beamlib.BEAM_EINVAL
+    assert L.beam_gpu_server_take(None, 1, None) == beamlib.BEAM_EINVAL
+    assert L.beam_gpu_server_memory(None, None, None) == beamlib.BEAM_EINVAL
 
 
 def test_host_cli_usage_and_errors(tmp_path):

@@ -1,0 +1,132 @@
+"""GPU tests of the job server (beam_gpu_server_*), through the C ABI. Needs an
+sm_100a device.
+
+Isolation: every job's bins are the same bit for bit whether it runs alone
+or among other jobs of other sizes and precisions admitted while it runs, and
+equal beam_gpu_run's. Admission: with a memory budget that holds one job's
+plan and buffers, jobs of two configurations still all finish, by evicting the
+idle plan. Failures: a job whose plan cannot be built ends FAILED with the
+plan's error."""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, golden_field
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(beamlib):
+    c = beamlib.Context(0)
+    yield c
+    c.close()
+
+
+def job_args(name, precision="fp64"):
+    NN, Nmax, Nr, UL, LL, BW, _ = GOLDEN_CASES[name]
+    return (NN, UL, LL, BW), dict(Nmax=Nmax, Nr=Nr, precision=precision)
+
+
+def fields(name, seeds):
+    from barbie_b200.synth import realization_seed, synth_field
+    return [synth_field(GOLDEN_CASES[name][0], realization_seed(r)) for r in seeds]
+
+
+def assert_same(got, want):
+    for k in ("bs", "norm", "out", "count"):
+        assert np.array_equal(got[k], want[k], equal_nan=True), k
+
+
+MIX = [("nn96_r20", "fp64"), ("nn256_cfg2", "fp64"), ("nn96_r20", "mixed"), ("nn64_bw2", "fp64"),
+       ("nn64_cfg1", "fp64")]
+
+
+def test_jobs_give_the_same_bins_alone_and_in_the_mix(beamlib, ctx):
+    work = []
+    for k, (name, prec) in enumerate(MIX):
+        for f in fields(name, (20 + k, 40 + k)):
+            work.append((name, prec, f))
+    # alone: one job on the device at a time
+    srv = beamlib.Server(ctx, max_active=1)
+    alone = []
+    for name, prec, f in work:
+        a, kw = job_args(name, prec)
+        j = srv.submit(f, *a, **kw)
+        assert srv.wait(j, 120000)["state"] == beamlib.JOB_DONE
+        alone.append(srv.take(j))
+    srv.close()
+    # the same as a plan's own run
+    a, kw = job_args(work[0][0], work[0][1])
+    plan = beamlib.Plan(ctx, *a, **kw)
+    assert_same(alone[0], plan.run(work[0][2]))
+    plan.close()
+    # in the mix: all submitted at once (twice over), up to four on the device
+    srv = beamlib.Server(ctx, max_active=4)
+    t0 = time.perf_counter()
+    ids = []
+    for rep in range(2):
+        for i, (name, prec, f) in enumerate(work):
+            a, kw = job_args(name, prec)
+            ids.append((i, time.perf_counter() - t0, srv.submit(f, *a, **kw)))
+    spans = []
+    for i, t_sub, j in ids:
+        info = srv.wait(j, 120000)
+        assert info["state"] == beamlib.JOB_DONE
+        got = srv.take(j)
+        assert_same(got, alone[i])
+        spans.append((t_sub * 1e3 + info["queue_ms"], t_sub * 1e3 + info["total_ms"]))
+    srv.close()
+    # jobs ran concurrently: some job started before another had finished
+    overlap = max(sum(1 for s, e in spans if s <= t < e) for t, _ in spans)
+    print(f"{len(spans)} jobs, at most {overlap} running at once")
+    assert overlap >= 2
+
+
+def test_memory_budget_admits_jobs_one_plan_at_a_time(beamlib, ctx):
+    sizes = {}
+    for name in ("nn96_r20", "nn64_cfg1"):
+        a, kw = job_args(name)
+        p = beamlib.Plan(ctx, *a, **kw)
+        sizes[name] = (p.info["device_bytes"], p.info["run_bytes"])
+        p.close()
+    biggest_plan = max(b for b, _ in sizes.values())
+    budget = int(1.2 * max(b + r for b, r in sizes.values()))
+    srv = beamlib.Server(ctx, mem_budget=budget, max_active=4)
+    want, ids = [], []
+    for k in range(3):
+        for name in ("nn96_r20", "nn64_cfg1"):
+            a, kw = job_args(name)
+            (f,) = fields(name, (60 + k,))
+            ids.append(srv.submit(f, *a, **kw))
+            p = beamlib.Plan(ctx, *a, **kw)
+            want.append(p.run(f))
+            p.close()
+    for j, w in zip(ids, want):
+        assert srv.wait(j, 120000)["state"] == beamlib.JOB_DONE
+        assert_same(srv.take(j), w)
+    now, peak = srv.memory()
+    srv.close()
+    # a plan's size is only known once built, so the peak may pass the budget by one plan
+    assert peak <= budget + biggest_plan, (peak, budget)
+
+
+def test_failed_jobs_report_their_error(beamlib, ctx):
+    srv = beamlib.Server(ctx)
+    NN = 64
+    f = np.zeros((NN, NN, NN + 2))
+    bad = srv.submit(f, NN, 11, 1, 1, Nmax=16, Nr=15)  # Nr must be a multiple of 10
+    info = srv.wait(bad, 120000)
+    assert info["state"] == beamlib.JOB_FAILED and info["error"] == beamlib.BEAM_EINVAL
+    with pytest.raises(beamlib.BeamError) as e:
+        srv.take(bad)
+    assert e.value.code == beamlib.BEAM_EINVAL
+    with pytest.raises(beamlib.BeamError) as e:
+        srv.wait(bad)
+    assert e.value.code == beamlib.BEAM_ENOTFOUND
+    good = srv.submit(f, NN, 11, 1, 1, Nmax=16, Nr=10)  # the server still works
+    assert srv.wait(good, 120000)["state"] == beamlib.JOB_DONE
+    res = srv.take(good)
+    assert np.all(res["count"] == 0)
+    srv.close()
