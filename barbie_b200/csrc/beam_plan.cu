@@ -284,6 +284,34 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   for (int u = 0; u < d.n_used; ++u)
     for (const Group &gr : groups[u]) total += (double)gr.ntiles * 256.0 * (double)(p->tri_first[u + 1] - p->tri_first[u]);
   const double target = std::max(1.0, total / (std::max(1, p->ctx->num_sms) * 8.0));
+  // Splits per triplet: by work (load balance) and by list length (no CTA
+  // walks more than about tau_max triangles: a CTA's time grows with its
+  // list, not its tiles). Each split keeps a partial sum per combo, so tau_max
+  // starts at TRI_TAU_MAX and doubles while the partial sums would pass
+  // max(PART_PER_COMBO x combos, PART_MIN) slots per realization.
+  constexpr long long PART_PER_COMBO = 4, PART_MIN = 64LL << 20;
+  std::vector<long long> nruns(d.n_used, 0);
+  std::vector<double> wmaxu(d.n_used, 0.0);
+  long long max_nt = 1;
+  for (int u = 0; u < d.n_used; ++u) {
+    if (!own[u]) continue;
+    const long long nt = p->tri_first[u + 1] - p->tri_first[u];
+    max_nt = std::max(max_nt, nt);
+    for (long long k = k2base[u]; k < k2base[u + 1]; ++k) nruns[u] += (k2cnt[k] > 0);
+    for (const Group &gr : groups[u]) wmaxu[u] = std::max(wmaxu[u], (double)gr.ntiles * 256.0 * (double)nt);
+  }
+  auto splits = [&](int u, long long tau_max) {
+    const long long nt = p->tri_first[u + 1] - p->tri_first[u];
+    double want = std::max(std::ceil(wmaxu[u] / target), std::ceil((double)nt / (double)tau_max));
+    return (int)std::min<double>(std::max(1.0, want), (double)std::max<long long>(1, nruns[u]));
+  };
+  long long tau_max = TRI_TAU_MAX;
+  for (;;) {
+    long long slots = 0;
+    for (int u = 0; u < d.n_used; ++u) slots += own[u] ? (long long)splits(u, tau_max) * u_ncombo[u] : u_ncombo[u];
+    if (slots <= std::max(PART_PER_COMBO * (long long)combo_p1.size(), PART_MIN) || tau_max >= max_nt) break;
+    tau_max *= 2;
+  }
   std::vector<TriChunk> chunks;
   std::vector<int2> pieces;
   std::vector<TriItem> items;
@@ -299,12 +327,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     std::vector<int2> runs;  // (length, k2)
     for (long long k = k2base[u]; k < k2base[u + 1]; ++k)
       if (k2cnt[k] > 0) runs.push_back(make_int2(k2cnt[k], (int)(k - k2base[u])));
-    double wmax = 0.0;
-    for (const Group &gr : groups[u]) wmax = std::max(wmax, (double)gr.ntiles * 256.0 * (double)nt);
-    // split by work (load balance) and by list length (no CTA walks more than
-    // about TRI_TAU_MAX triangles: a CTA's time grows with its list, not its tiles)
-    double want = std::max(std::ceil(wmax / target), std::ceil((double)nt / TRI_TAU_MAX));
-    int ns = (int)std::min<double>(std::max(1.0, want), std::max<size_t>(1, runs.size()));
+    int ns = splits(u, tau_max);
     u_nsplit[u] = ns;
     u_part[u + 1] = u_part[u] + (long long)ns * u_ncombo[u];
     int rp = p->used_rp[u];

@@ -54,7 +54,18 @@ def parse_args():
     ap.add_argument("--fields", type=int, default=2, help="realizations per rank, cycled over the steps")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched form (64 realizations at NN=256)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving form (Poisson job stream)")
+    ap.add_argument("--serve-jobs", type=int, default=40, help="jobs per precision in the serving stream")
+    ap.add_argument("--batch-pool", type=int, default=8, help="distinct fields cycled over the batch")
     return ap.parse_args()
+
+
+# batched form: 64 realizations of the field recipe at NN=256, Nr=30 rings, mixed precision
+BATCH = dict(NN=256, Nmax=64, Nr=30, UL_k1=31, LL_k1=1, BW_k1=1, n_mtbin=5, realizations=64)
+# serving form: NN -> (Nmax, Nr) with the ring extent Nmax below NN/3 and above the
+# last ring's lower edge (27.9, 56.9, 95.9 for Nr = 20, 30, 40); bins 1..Nmax of width 1 or 2
+SERVE = {128: (40, 20), 192: (60, 30), 256: (64, 30), 384: (100, 40), 512: (128, 40)}
 
 
 # --------------------------------------------------------------------- clocks
@@ -273,6 +284,8 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_port(fields[0], info)
+    batched = run_batched(ctx, args) if world == 1 and not args.no_batch else None
+    serving = run_serving(ctx, args) if world == 1 and not args.no_serve else None
 
     # kernels per bispectrum as the library counted them in the last run: mode
     # build, one triangle-sum launch per tile class, split reduction, epilogue
@@ -290,7 +303,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps},
         "latency": lat, "wall_s": wall, "clocks": clk, "roofline": roofline, "mixed": mixed,
-        "cpu_baseline": cpu, "gpu_launches": gpu_launches,
+        "cpu_baseline": cpu, "gpu_launches": gpu_launches, "batched": batched, "serving": serving,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -298,6 +311,103 @@ def run_ours(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_batched(ctx, args):
+    """The batched form: BATCH['realizations'] host fields through
+    beam_gpu_run_batch (one launch per kernel over each batch, replayed CUDA
+    graphs, host gather of batch i+1 overlapping the device work of batch i),
+    timed end to end on the host clock, against the same fields one
+    beam_gpu_run call at a time."""
+    from barbie_b200 import beam
+    from barbie_b200.synth import realization_seed, synth_field
+    B = BATCH
+    pool = [synth_field(B["NN"], realization_seed(r)) for r in range(1, args.batch_pool + 1)]
+    fields = [pool[i % len(pool)] for i in range(B["realizations"])]
+    out = {"workload": f"{B['realizations']} realizations at NN={B['NN']}, Nmax={B['Nmax']}, Nr={B['Nr']}, "
+                       f"k1 bins 1..{B['UL_k1']} width 1",
+           "fields": f"{len(pool)} distinct seeded fields cycled over the {B['realizations']} realizations",
+           "timing": "host wall clock around each call (host gather, H2D, kernels, D2H of the bins)"}
+    for prec in ("mixed", "fp64"):
+        plan = beam.Plan(ctx, B["NN"], B["UL_k1"], B["LL_k1"], B["BW_k1"], Nmax=B["Nmax"], Nr=B["Nr"],
+                         n_mtbin=B["n_mtbin"], precision=prec)
+        res = {}
+        for label, batch in (("batched", 0), ("batch_of_16", 16)):
+            plan.run_batch(fields, batch=batch)  # warm-up: slots and graphs
+            t = []
+            for _ in range(max(1, args.steps // 3)):
+                t0 = time.perf_counter()
+                plan.run_batch(fields, batch=batch)
+                t.append(time.perf_counter() - t0)
+            res[label] = {"value": len(fields) / min(t) * 3600.0, "seconds_per_call": min(t)}
+        for f in pool[:2]:
+            plan.run(f)
+        t0 = time.perf_counter()
+        for f in fields:
+            plan.run(f)
+        res["one_at_a_time"] = {"value": len(fields) / (time.perf_counter() - t0) * 3600.0}
+        res["unit"] = UNIT
+        res["batch_speedup"] = res["batched"]["value"] / res["one_at_a_time"]["value"]
+        res["device_bytes"] = plan.refresh_info()["device_bytes"]
+        out[prec] = res
+        plan.close()
+    return out
+
+
+def run_serving(ctx, args):
+    """The serving form: a Poisson stream of jobs, each one realization with NN
+    drawn from SERVE, bins of width 1 or 2, through the job server (admission
+    by device-memory footprint, up to 4 jobs on the device at once). Reports
+    per-job latency (submission to bins on the host) and throughput, for the
+    plain and the mixed path."""
+    from barbie_b200 import beam
+    from barbie_b200.synth import realization_seed, synth_field
+    rng = np.random.default_rng(500)
+    nns = sorted(SERVE)
+    pool = {NN: synth_field(NN, realization_seed(1000 + NN)) for NN in nns}
+    jobs = [(int(rng.choice(nns)), int(rng.choice([1, 2]))) for _ in range(args.serve_jobs)]
+    gaps = rng.exponential(1.0, size=len(jobs))  # unit-mean gaps, scaled to the rate below
+    out = {"workload": f"{len(jobs)} jobs per path, NN uniform over {nns}, (Nmax, Nr) = "
+                       f"{ {k: v for k, v in SERVE.items()} }, k1 bins 1..Nmax width 1 or 2, 5 t x 5 mu bins",
+           "arrivals": "Poisson at 70% of the mean single-job service rate measured in the warm-up",
+           "fields": "one seeded field per NN (job r2c buffers are read from host memory per job)",
+           "latency": "submission to bins in host memory, host clock"}
+    for prec in ("fp64", "mixed"):
+        srv = beam.Server(ctx, max_active=4)
+        service = {}
+        for NN, BW in sorted(set(jobs)):  # warm-up: builds and caches the plans, one job per configuration
+            Nmax, Nr = SERVE[NN]
+            j = srv.submit(pool[NN], NN, Nmax + 1, 1, BW, Nmax=Nmax, Nr=Nr, precision=prec)
+            info = srv.wait(j, 600000)
+            srv.take(j)
+            service[(NN, BW)] = info["run_ms"] / 1e3
+        mean_service = float(np.mean([service[k] for k in jobs]))
+        rate = 0.7 / mean_service
+        ids = []
+        t0 = time.perf_counter()
+        t_next = t0
+        for (NN, BW), g in zip(jobs, gaps):
+            t_next += g / rate
+            dt = t_next - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            Nmax, Nr = SERVE[NN]
+            ids.append(srv.submit(pool[NN], NN, Nmax + 1, 1, BW, Nmax=Nmax, Nr=Nr, precision=prec))
+        lat, run = [], []
+        for j in ids:
+            info = srv.wait(j, 600000)
+            srv.take(j)
+            lat.append(info["total_ms"])
+            run.append(info["run_ms"])
+        wall = time.perf_counter() - t0
+        _, peak = srv.memory()
+        srv.close()
+        out[prec] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "max_ms": float(np.max(lat)), "service_p50_ms": float(np.percentile(run, 50)),
+                     "throughput": len(jobs) / wall * 3600.0, "unit": UNIT, "arrival_rate_per_s": rate,
+                     "mean_service_alone_s": mean_service, "peak_device_bytes": peak,
+                     "service_alone_ms": {f"NN{k[0]}_BW{k[1]}": v * 1e3 for k, v in sorted(service.items())}}
+    return out
 
 
 def cpu_baseline_port(field, info):
