@@ -198,6 +198,24 @@ int beam_gpu_plan_get_info(const beam_gpu_plan *p, beam_plan_info *info) {
   return BEAM_OK;
 }
 
+// Host gather of one realization's mode rows, split over up to 8 host threads
+// when there is more than about a megabyte to move.
+static void gather_one(const beam_gpu_plan *p, RunSlot *s, const double *r2c) {
+  const int nm = p->d.n_modes;
+  const size_t bytes = (size_t)nm * p->d.Q * 16;
+  unsigned hw = std::thread::hardware_concurrency();
+  int nt = (int)std::min<size_t>(std::min<unsigned>(std::max(1u, hw), 8u), bytes >> 20);
+  if (nt <= 1) {
+    gather_host(p, s, 0, r2c);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int k = 1; k < nt; ++k)
+    th.emplace_back([=]() { gather_host(p, s, 0, r2c, (int)((long long)nm * k / nt), (int)((long long)nm * (k + 1) / nt)); });
+  gather_host(p, s, 0, r2c, 0, nm / nt);
+  for (std::thread &t : th) t.join();
+}
+
 // Triangle sums of one realization on the plan's own slot.
 static int compute_B(beam_gpu_plan *p, const double *r2c, int on_device) {
   RunSlot *s = p->main;
@@ -209,7 +227,7 @@ static int compute_B(beam_gpu_plan *p, const double *r2c, int on_device) {
     s->h_src[s->cap] = r2c;
     BEAM_TRY(upload_modes(p, s, 1, false));
   } else {
-    gather_host(p, s, 0, r2c);
+    gather_one(p, s, r2c);
     BEAM_TRY(upload_modes(p, s, 1, true));
   }
   return run_triangle_sums(p, s, 1);

@@ -79,6 +79,12 @@ struct TriDesc {
 static_assert(sizeof(TriDesc) % 16 == 0 && TRI_CHUNK <= 31 && TRI_PIECES <= 4, "TriDesc layout");
 constexpr int TRI_TAU_MAX = 512;  // most in-plane triangles walked by one CTA
 
+// Shared-memory pitch (complex values) of a staged x or z row of L values.
+// The FP64 consumer reads a quarter-warp's 8 lanes as 2 planes x 4 rows with
+// 16-byte loads; rows 2 (mod 8) 16-byte units apart put those 8 lanes on
+// distinct banks. The mixed-precision consumer reads rows as staged.
+__host__ __device__ inline int stage_pitch(int L, bool fp64) { return fp64 ? L + ((2 - L) & 7) : L; }
+
 // One CTA of triangle-sum work: tiles [tile0, tile0 + ntiles) of ring triplet u
 // over chunks [ch0, ch1) (the triplet's split `split`). Rows staged per chunk
 // are columns [colx, colx+Lx) of ring r1's mode rows (one per triangle),
@@ -219,7 +225,7 @@ size_t slot_bytes(const beam_gpu_plan *p, int cap);
 int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out);
 void slot_destroy(RunSlot *s);
 // per-realization steps on a slot, for realizations [0, n) (beam_run.cu)
-void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c);
+void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c, int m0 = 0, int m1 = -1);
 int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged);
 int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n);
 int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n);

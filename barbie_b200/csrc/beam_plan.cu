@@ -441,7 +441,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   for (int n = 0; n <= TRI_WARPS; ++n) d.class_stage[n] = 0;
   for (const TriItem &it : sorted) {
     d.class_first[it.ntiles + 1]++;
-    int stage = TRI_CHUNK * (it.Lx + it.Lz) + TRI_PIECES * it.Ly;
+    const bool f64 = (A == 1);
+    int stage = TRI_CHUNK * (stage_pitch(it.Lx, f64) + stage_pitch(it.Lz, f64)) + TRI_PIECES * it.Ly;
     d.class_stage[it.ntiles] = std::max(d.class_stage[it.ntiles], stage);
   }
   for (int n = 0; n <= TRI_WARPS; ++n) d.class_first[n + 1] += d.class_first[n];

@@ -292,14 +292,15 @@ int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out) {
   return BEAM_OK;
 }
 
-// Copy the plan's mode rows of one host r2c buffer into the slot's pinned
-// staging rows of realization r (funcs.c:94-106 reads the same elements).
-void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c) {
+// Copy the plan's mode rows [m0, m1) of one host r2c buffer into the slot's
+// pinned staging rows of realization r (funcs.c:94-106 reads the same elements).
+void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c, int m0, int m1) {
   const DevPlan &d = p->d;
   const long NN = p->geom.NN, NH = NN / 2 + 1;
   const int Q = d.Q;
   double *dst = s->h_staging + (size_t)2 * r * d.n_modes * Q;
-  for (int m = 0; m < d.n_modes; ++m) {
+  if (m1 < 0 || m1 > d.n_modes) m1 = d.n_modes;
+  for (int m = m0; m < m1; ++m) {
     size_t row = ((size_t)p->mode_ij[2 * m] * NN + (size_t)p->mode_ij[2 * m + 1]) * (size_t)NH;
     std::memcpy(dst + (size_t)2 * m * Q, r2c + 2 * row, sizeof(double) * 2 * Q);
   }

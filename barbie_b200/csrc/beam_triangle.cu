@@ -13,10 +13,14 @@
 // of k2 over its planes p2 -- completing on full[s] (transaction bytes). Each
 // consumer releases a stage on empty[s]; the producer refills it when all have.
 //
-// A consumer thread owns the combos (p1_0 + q, p3_0 + lane), q < TRI_P1, of
-// its tile. Over a piece it accumulates w[q] += x_{k1}(p1_0+q) * z_{k3}(p3)
-// (4 FMA; x read warp-wide from one address) and at the end of the piece adds
-// Re(y_{k2}(-p1_0-q-p3) * w[q]) to its sums.
+// A consumer warp accumulates, over each piece (one k2), the complex outer
+// product w(p1, p3) += x_{k1}(p1) z_{k3}(p3) of its tile and at the end of the
+// piece adds Re(y_{k2}(-p1-p3) w(p1, p3)) to the tile's sums. The FP64 path
+// forms the outer products on the FP64 tensor cores (tri_consume_dmma: five
+// 128-bit shared loads per warp for 4096 FMA), the mixed path with FP32 FMA
+// and x broadcast (tri_consume_fma).
+#include <type_traits>
+
 #include "beam_device.cuh"
 #include "beam_internal.h"
 
@@ -75,17 +79,213 @@ __device__ __forceinline__ void tri_issue(const TriArgs &a, const TriItem &it, c
                                           const TriMeta &m) {
   const int lane = threadIdx.x & 31;
   const int nt = chunk_nt(m.packed), npc = chunk_npc(m.packed);
-  C *xs = st, *zs = st + TRI_CHUNK * it.Lx, *ys = zs + TRI_CHUNK * it.Lz;
+  constexpr bool F64 = std::is_same<C, double2>::value;
+  const int px = stage_pitch(it.Lx, F64), pz = stage_pitch(it.Lz, F64);
+  C *xs = st, *zs = st + TRI_CHUNK * px, *ys = zs + TRI_CHUNK * pz;
   if (lane == 0) mbar_expect_tx(full, (uint32_t)((nt * (it.Lx + it.Lz) + npc * it.Ly) * sizeof(C)));
   __syncwarp();
   if (lane < nt) {
     const int mx = it.m1 + (int)(m.xz & 0xffffu), mz = it.m3 + (int)(m.xz >> 16);
-    bulk_g2s(smem_addr(xs + lane * it.Lx), S + (size_t)mx * a.W + it.colx, (uint32_t)(it.Lx * sizeof(C)), full);
-    bulk_g2s(smem_addr(zs + lane * it.Lz), S + (size_t)mz * a.W + it.colz, (uint32_t)(it.Lz * sizeof(C)), full);
+    bulk_g2s(smem_addr(xs + lane * px), S + (size_t)mx * a.W + it.colx, (uint32_t)(it.Lx * sizeof(C)), full);
+    bulk_g2s(smem_addr(zs + lane * pz), S + (size_t)mz * a.W + it.colz, (uint32_t)(it.Lz * sizeof(C)), full);
   }
   if (lane < npc)
     bulk_g2s(smem_addr(ys + lane * it.Ly), S + (size_t)(it.m2 + m.y) * a.W + it.coly, (uint32_t)(it.Ly * sizeof(C)),
              full);
+}
+
+// Wait until chunk c has landed in its stage; false (status set) when the
+// bounded wait gave up or another warp's did.
+__device__ __forceinline__ bool tri_wait_chunk(const TriArgs &a, uint64_t *full, volatile int *s_fail, int c,
+                                               int lane) {
+  if (*s_fail || !mbar_wait_bounded(smem_addr(&full[c % TRI_STAGES]), (uint32_t)((c / TRI_STAGES) & 1))) {
+    *s_fail = 1;
+    if (lane == 0) atomicOr(a.status, DEV_TIMEOUT);
+    return false;
+  }
+  return true;
+}
+
+// Partial-sum slots of this CTA's item (split `it.split`) for realization blockIdx.y.
+__device__ __forceinline__ double *tri_out(const TriArgs &a, const TriItem &it) {
+  const int nc = a.u_ncombo[it.u];
+  return a.part + (long long)blockIdx.y * a.part_stride + a.u_part[it.u] + (long long)it.split * nc -
+         a.u_cfirst[it.u];
+}
+
+// FMA consumer (mixed precision). A thread owns the combos (p1_0 + q,
+// p3_0 + lane), q < TRI_P1, of its tile. Over a piece it accumulates
+// w[q] += x_k1(p1_0+q) * z_k3(p3) (4 FMA; x read warp-wide from one address)
+// and at the end of the piece adds Re(y_k2(-p1_0-q-p3) * w[q]) to its sums.
+template <typename C>
+__device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem &it, const C *stages, uint64_t *full,
+                                                uint64_t *empty, volatile int *s_fail, int warp, int lane,
+                                                int nch) {
+  typedef typename TriAcc<C>::t acc_t;
+  const TriTile tl = a.tiles[it.tile0 + warp];
+  const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + lane;
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < TRI_P1; ++q) any |= (tc[q * 32] >= 0);
+  const int p3 = tl.p3_0 + lane;
+  const int ox0 = tl.p1_0 + a.colbase - it.colx;                          // x reads ox0 + q
+  const int oz = any ? p3 + a.colbase - it.colz : 0;                      // z read
+  const int oy0 = any ? -tl.p1_0 - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
+  double sum[TRI_P1];
+#pragma unroll
+  for (int q = 0; q < TRI_P1; ++q) sum[q] = 0.0;
+  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
+  for (int c = 0; c < nch; ++c) {
+    const int s = c % TRI_STAGES;
+    const int packed = packed_next;  // piece layout of this chunk, loaded one chunk ahead
+    if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
+    if (!tri_wait_chunk(a, full, s_fail, c, lane)) return;
+    const C *xs = stages + s * a.stage;
+    const C *zs = xs + TRI_CHUNK * it.Lx;
+    const C *ys = zs + TRI_CHUNK * it.Lz;
+    const int npc = chunk_npc(packed);
+    int tt = 0;
+    for (int pc = 0; pc < npc; ++pc) {
+      const int len = chunk_len(packed, pc);
+      acc_t wr[TRI_P1], wi[TRI_P1];
+#pragma unroll
+      for (int q = 0; q < TRI_P1; ++q) wr[q] = wi[q] = (acc_t)0;
+      for (int j = 0; j < len; ++j, ++tt) {
+        const C z = zs[tt * it.Lz + oz];
+        const C *xr = xs + tt * it.Lx + ox0;
+        // x in two halves: the empty asm keeps the compiler from holding all
+        // TRI_P1 values at once, which leaves the sums room in registers
+#pragma unroll
+        for (int h = 0; h < TRI_P1; h += TRI_P1 / 2) {
+#pragma unroll
+          for (int q = h; q < h + TRI_P1 / 2; ++q) {
+            const C x = xr[q];
+            wr[q] = fma(x.x, z.x, fma(-x.y, z.y, wr[q]));
+            wi[q] = fma(x.x, z.y, fma(x.y, z.x, wi[q]));
+          }
+          asm volatile("" ::: "memory");
+        }
+      }
+      const C *yr = ys + pc * it.Ly + oy0;
+#pragma unroll
+      for (int q = 0; q < TRI_P1; ++q) {
+        const C y = yr[-q];
+        sum[q] += (double)fma(y.x, wr[q], -y.y * wi[q]);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
+  }
+  double *out = tri_out(a, it);
+#pragma unroll
+  for (int q = 0; q < TRI_P1; ++q) {
+    const int cidx = tc[q * 32];
+    if (cidx >= 0) out[cidx] = sum[q];
+  }
+}
+
+// D += A * B for one 8x8x4 FP64 tile on the tensor cores (mma.sync m8n8k4,
+// the FP64 MMA of sm_80 and later; tcgen05 has no FP64 kind). Lane l holds
+// a = A[l/4][l%4], b = B[l%4][l/4] and d0, d1 = D[l/4][2*(l%4)], D[l/4][2*(l%4)+1].
+__device__ __forceinline__ void dmma884(double &d0, double &d1, double av, double bv) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(av), "d"(bv));
+}
+
+// FP64 consumer on the FP64 tensor cores. The warp's tile of TRI_P1 = 8
+// planes p1 x 32 planes p3 is four 8x8 blocks n. Per group of four triangles
+// of a piece, every block gets W_n += X Z_n^T in complex arithmetic as four
+// real m8n8k4 MMAs (Wr += Xr Zr^T - Xi Zi^T, Wi += Xr Zi^T + Xi Zr^T). Lane l
+// supplies x of plane p1_0 + l/4 and z of plane p3_0 + 8n + l/4 for triangle
+// l%4 of the group (zero past the piece's end) and holds the W entries of
+// combos (p1_0 + l/4, p3_0 + 8n + 2(l%4) + e), e < 2. At the end of the piece
+// each such entry adds Re(y_k2(-p1-p3) * W) to its sum. Per group of four
+// triangles a warp makes 5 128-bit shared loads for 4096 FMA.
+__device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem &it, const double2 *stages,
+                                                 uint64_t *full, uint64_t *empty, volatile int *s_fail, int warp,
+                                                 int lane, int nch) {
+  static_assert(TRI_P1 == 8, "the DMMA consumer tiles 8 planes p1");
+  const TriTile tl = a.tiles[it.tile0 + warp];
+  const int g = lane >> 2, t = lane & 3;
+  const int px = stage_pitch(it.Lx, true), pz = stage_pitch(it.Lz, true);  // staged row pitches
+  const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + g * 32 + 2 * t;
+  const int ox = tl.p1_0 + g + a.colbase - it.colx;  // inside the staged x row for every lane
+  // z of planes outside the staged p3 range and y of combos outside the staged
+  // p2 range read column 0 instead (those combos' sums are never stored)
+  int oz[4];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    const int o = tl.p3_0 + 8 * n + g + a.colbase - it.colz;
+    oz[n] = (unsigned)o < (unsigned)it.Lz ? o : 0;
+  }
+  const int oyb = -(tl.p1_0 + g) - (tl.p3_0 + 2 * t) + a.colbase - it.coly;  // y of (n, e): oyb - 8n - e
+  double sum[4][2];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) sum[n][0] = sum[n][1] = 0.0;
+  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
+  for (int c = 0; c < nch; ++c) {
+    const int s = c % TRI_STAGES;
+    const int packed = packed_next;
+    if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
+    if (!tri_wait_chunk(a, full, s_fail, c, lane)) return;
+    const double2 *xs = stages + s * a.stage;
+    const double2 *zs = xs + TRI_CHUNK * px;
+    const double2 *ys = zs + TRI_CHUNK * pz;
+    const int npc = chunk_npc(packed);
+    int tt = 0;
+    for (int pc = 0; pc < npc; ++pc) {
+      const int len = chunk_len(packed, pc);
+      double wr[4][2], wi[4][2];
+#pragma unroll
+      for (int n = 0; n < 4; ++n) wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
+      for (int k0 = 0; k0 < len; k0 += 4) {
+        const bool on = k0 + t < len;
+        const int row = tt + (on ? k0 + t : 0);
+        double2 xv = xs[row * px + ox];
+        if (!on) xv = make_double2(0.0, 0.0);
+        double2 zv[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          zv[n] = zs[row * pz + oz[n]];
+          if (!on) zv[n] = make_double2(0.0, 0.0);
+        }
+        // first the products of the real parts of x, then those of the
+        // imaginary parts: each accumulator's two MMAs are eight apart
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          dmma884(wr[n][0], wr[n][1], xv.x, zv[n].x);
+          dmma884(wi[n][0], wi[n][1], xv.x, zv[n].y);
+        }
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          dmma884(wr[n][0], wr[n][1], -xv.y, zv[n].y);
+          dmma884(wi[n][0], wi[n][1], xv.y, zv[n].x);
+        }
+      }
+      tt += len;
+      const double2 *yr = ys + pc * it.Ly;
+#pragma unroll
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          int o = oyb - 8 * n - e;
+          o = (unsigned)o < (unsigned)it.Ly ? o : 0;
+          const double2 y = yr[o];
+          sum[n][e] += fma(y.x, wr[n][e], -y.y * wi[n][e]);
+        }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
+  }
+  double *out = tri_out(a, it);
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int cidx = tc[8 * n + e];
+      if (cidx >= 0) out[cidx] = sum[n][e];
+    }
 }
 
 template <typename C>
@@ -139,74 +339,10 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
   }
 
   // -------------------------------------------------------------- consumer
-  // columns of this thread's reads in the staged rows
-  const TriTile tl = a.tiles[it.tile0 + warp];
-  const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + lane;
-  bool any = false;
-#pragma unroll
-  for (int q = 0; q < TRI_P1; ++q) any |= (tc[q * 32] >= 0);
-  const int p3 = tl.p3_0 + lane;
-  const int ox0 = tl.p1_0 + a.colbase - it.colx;                          // x reads ox0 + q
-  const int oz = any ? p3 + a.colbase - it.colz : 0;                      // z read
-  const int oy0 = any ? -tl.p1_0 - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
-  double sum[TRI_P1];
-#pragma unroll
-  for (int q = 0; q < TRI_P1; ++q) sum[q] = 0.0;
-
-  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
-  for (int c = 0; c < nch; ++c) {
-    const int s = c % TRI_STAGES;
-    const int packed = packed_next;  // piece layout of this chunk, loaded one chunk ahead
-    if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
-    if (s_fail || !mbar_wait_bounded(smem_addr(&full[s]), (uint32_t)((c / TRI_STAGES) & 1))) {
-      s_fail = 1;
-      if (lane == 0) atomicOr(a.status, DEV_TIMEOUT);
-      return;
-    }
-    const C *xs = stages + s * a.stage;
-    const C *zs = xs + TRI_CHUNK * it.Lx;
-    const C *ys = zs + TRI_CHUNK * it.Lz;
-    const int npc = chunk_npc(packed);
-    int tt = 0;
-    for (int pc = 0; pc < npc; ++pc) {
-      const int len = chunk_len(packed, pc);
-      acc_t wr[TRI_P1], wi[TRI_P1];
-#pragma unroll
-      for (int q = 0; q < TRI_P1; ++q) wr[q] = wi[q] = (acc_t)0;
-      for (int j = 0; j < len; ++j, ++tt) {
-        const C z = zs[tt * it.Lz + oz];
-        const C *xr = xs + tt * it.Lx + ox0;
-        // x in two halves: the empty asm keeps the compiler from holding all
-        // TRI_P1 values at once, which leaves the sums room in registers
-#pragma unroll
-        for (int h = 0; h < TRI_P1; h += TRI_P1 / 2) {
-#pragma unroll
-          for (int q = h; q < h + TRI_P1 / 2; ++q) {
-            const C x = xr[q];
-            wr[q] = fma(x.x, z.x, fma(-x.y, z.y, wr[q]));
-            wi[q] = fma(x.x, z.y, fma(x.y, z.x, wi[q]));
-          }
-          asm volatile("" ::: "memory");
-        }
-      }
-      const C *yr = ys + pc * it.Ly + oy0;
-#pragma unroll
-      for (int q = 0; q < TRI_P1; ++q) {
-        const C y = yr[-q];
-        sum[q] += (double)fma(y.x, wr[q], -y.y * wi[q]);
-      }
-    }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
-  }
-  const int nc = a.u_ncombo[it.u];
-  double *out = a.part + (long long)blockIdx.y * a.part_stride + a.u_part[it.u] + (long long)it.split * nc -
-                a.u_cfirst[it.u];
-#pragma unroll
-  for (int q = 0; q < TRI_P1; ++q) {
-    const int cidx = tc[q * 32];
-    if (cidx >= 0) out[cidx] = sum[q];
-  }
+  if constexpr (std::is_same<C, double2>::value)
+    tri_consume_dmma(a, it, stages, full, empty, &s_fail, warp, lane, nch);
+  else
+    tri_consume_fma<C>(a, it, stages, full, empty, &s_fail, warp, lane, nch);
 }
 
 // Sum the splits of each combo in split order, scale by NN^2 and store the
