@@ -52,8 +52,12 @@ constexpr int TRI_PIECES = 4;  // pieces per stage
 constexpr int TRI_STAGES = 3;  // pipeline depth
 constexpr int TRI_PAD = 8;     // zero columns on each side of a mode row (>= TRI_P1 - 1)
 
+// A warp's tile: TRI_BLOCKS blocks of TRI_P1 planes p1 x TRI_BW planes p3 of
+// one ring triplet; tile column TRI_BW * n + c is plane p3_0[n] + c, tile row
+// a of block n plane p1_0[n] + a.
+constexpr int TRI_BW = 8, TRI_BLOCKS = 32 / TRI_BW;
 struct TriTile {
-  int p1_0, p3_0;  // planes p1_0 + a (a < TRI_P1) and p3_0 + lane
+  int p1_0[TRI_BLOCKS], p3_0[TRI_BLOCKS];
 };
 
 struct TriChunk {

@@ -243,9 +243,11 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     std::vector<Slot> slots(nc);
     for (int k = 0; k < nc; ++k) {
       int c = cf + k, p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
-      long long bp1 = p1 / TRI_P1, bp3 = (p3 - p3min) / 32;
-      // a group is one window of 32 planes p3 over up to TRI_WARPS blocks of planes p1
-      slots[k] = Slot{bp3 * 1000000 + bp1 / TRI_WARPS, bp1 * 1000000 + bp3, p1 % TRI_P1, (p3 - p3min) % 32, c};
+      long long bp1 = p1 / TRI_P1, b3 = (p3 - p3min) / TRI_BW;
+      // a group is one window of 32 planes p3 over up to TRI_WARPS blocks of
+      // planes p1; its non-empty TRI_P1 x TRI_BW blocks are packed four to a tile
+      slots[k] = Slot{(b3 / TRI_BLOCKS) * 1000000 + bp1 / TRI_WARPS, bp1 * 1000000 + b3, p1 % TRI_P1,
+                      (p3 - p3min) % TRI_BW, c};
     }
     std::sort(slots.begin(), slots.end(), [](const Slot &x, const Slot &y) {
       return x.gkey != y.gkey ? x.gkey < y.gkey : (x.tkey != y.tkey ? x.tkey < y.tkey : x.c < y.c);
@@ -255,21 +257,32 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
                1 << 30, -(1 << 30)};
       long long gk = slots[k].gkey;
       while (k < slots.size() && slots[k].gkey == gk) {
-        long long tk = slots[k].tkey;
-        int bp1 = (int)(tk / 1000000), bp3 = (int)(tk % 1000000);
-        tiles.push_back(TriTile{bp1 * TRI_P1, p3min + bp3 * 32});
+        TriTile tl;
+        tiles.push_back(tl);
         tile_combo.resize(tiles.size() * TRI_P1 * 32, -1);
         int32_t *tc = tile_combo.data() + (tiles.size() - 1) * TRI_P1 * 32;
-        for (; k < slots.size() && slots[k].tkey == tk && slots[k].gkey == gk; ++k) {
-          const Slot &s = slots[k];
-          tc[s.a * 32 + s.lane] = s.c;
-          int p1 = combo_p1[s.c], p2 = combo_p2[s.c], p3 = -p1 - p2;
-          gr.p1lo = std::min(gr.p1lo, p1); gr.p1hi = std::max(gr.p1hi, p1);
-          gr.p2lo = std::min(gr.p2lo, p2); gr.p2hi = std::max(gr.p2hi, p2);
-          gr.p3lo = std::min(gr.p3lo, p3); gr.p3hi = std::max(gr.p3hi, p3);
+        int nb = 0;
+        for (; nb < TRI_BLOCKS && k < slots.size() && slots[k].gkey == gk; ++nb) {
+          long long bk = slots[k].tkey;
+          int bp1 = (int)(bk / 1000000), b3 = (int)(bk % 1000000);
+          tl.p1_0[nb] = bp1 * TRI_P1;
+          tl.p3_0[nb] = p3min + b3 * TRI_BW;
+          for (; k < slots.size() && slots[k].tkey == bk && slots[k].gkey == gk; ++k) {
+            const Slot &s = slots[k];
+            tc[s.a * 32 + nb * TRI_BW + s.lane] = s.c;
+            int p1 = combo_p1[s.c], p2 = combo_p2[s.c], p3 = -p1 - p2;
+            gr.p1lo = std::min(gr.p1lo, p1); gr.p1hi = std::max(gr.p1hi, p1);
+            gr.p2lo = std::min(gr.p2lo, p2); gr.p2hi = std::max(gr.p2hi, p2);
+            gr.p3lo = std::min(gr.p3lo, p3); gr.p3hi = std::max(gr.p3hi, p3);
+          }
+          gr.tp1lo = std::min(gr.tp1lo, bp1 * TRI_P1);
+          gr.tp1hi = std::max(gr.tp1hi, bp1 * TRI_P1);
         }
-        gr.tp1lo = std::min(gr.tp1lo, bp1 * TRI_P1);
-        gr.tp1hi = std::max(gr.tp1hi, bp1 * TRI_P1);
+        for (int n = nb; n < TRI_BLOCKS; ++n) {  // unused blocks repeat the first one (no combos)
+          tl.p1_0[n] = tl.p1_0[0];
+          tl.p3_0[n] = tl.p3_0[0];
+        }
+        tiles.back() = tl;
         gr.ntiles++;
       }
       if (gr.ntiles > TRI_WARPS) {

@@ -122,15 +122,16 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
                                                 uint64_t *empty, volatile int *s_fail, int warp, int lane,
                                                 int nch) {
   typedef typename TriAcc<C>::t acc_t;
-  const TriTile tl = a.tiles[it.tile0 + warp];
   const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + lane;
   bool any = false;
 #pragma unroll
   for (int q = 0; q < TRI_P1; ++q) any |= (tc[q * 32] >= 0);
-  const int p3 = tl.p3_0 + lane;
-  const int ox0 = tl.p1_0 + a.colbase - it.colx;                          // x reads ox0 + q
-  const int oz = any ? p3 + a.colbase - it.colz : 0;                      // z read
-  const int oy0 = any ? -tl.p1_0 - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
+  // the lane's block nb: planes p1_0[nb] + q and p3 = p3_0[nb] + lane % TRI_BW
+  const int nb = lane / TRI_BW;
+  const int p1b = a.tiles[it.tile0 + warp].p1_0[nb], p3 = a.tiles[it.tile0 + warp].p3_0[nb] + lane % TRI_BW;
+  const int ox0 = p1b + a.colbase - it.colx;                          // x reads ox0 + q
+  const int oz = any ? p3 + a.colbase - it.colz : 0;                  // z read
+  const int oy0 = any ? -p1b - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
   double sum[TRI_P1];
 #pragma unroll
   for (int q = 0; q < TRI_P1; ++q) sum[q] = 0.0;
@@ -193,15 +194,15 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double av, doubl
       : "d"(av), "d"(bv));
 }
 
-// FP64 consumer on the FP64 tensor cores. The warp's tile of TRI_P1 = 8
-// planes p1 x 32 planes p3 is four 8x8 blocks n. Per group of four triangles
-// of a piece, every block gets W_n += X Z_n^T in complex arithmetic as four
-// real m8n8k4 MMAs (Wr += Xr Zr^T - Xi Zi^T, Wi += Xr Zi^T + Xi Zr^T). Lane l
-// supplies x of plane p1_0 + l/4 and z of plane p3_0 + 8n + l/4 for triangle
+// FP64 consumer on the FP64 tensor cores. The warp's tile is four blocks n of
+// 8 planes p1 x 8 planes p3 (TriTile). Per group of four triangles of a
+// piece, every block gets W_n += X_n Z_n^T in complex arithmetic as four real
+// m8n8k4 MMAs (Wr += Xr Zr^T - Xi Zi^T, Wi += Xr Zi^T + Xi Zr^T). Lane l
+// supplies x of plane p1_0[n] + l/4 and z of plane p3_0[n] + l/4 for triangle
 // l%4 of the group (zero past the piece's end) and holds the W entries of
-// combos (p1_0 + l/4, p3_0 + 8n + 2(l%4) + e), e < 2. At the end of the piece
-// each such entry adds Re(y_k2(-p1-p3) * W) to its sum. Per group of four
-// triangles a warp makes 5 128-bit shared loads for 4096 FMA.
+// combos (p1_0[n] + l/4, p3_0[n] + 2(l%4) + e), e < 2. At the end of the
+// piece each such entry adds Re(y_k2(-p1-p3) * W) to its sum. Per group of
+// four triangles a warp makes 8 128-bit shared loads for 4096 FMA.
 __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem &it, const double2 *stages,
                                                  uint64_t *full, uint64_t *empty, volatile int *s_fail, int warp,
                                                  int lane, int nch) {
@@ -210,16 +211,18 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
   const int g = lane >> 2, t = lane & 3;
   const int px = stage_pitch(it.Lx, true), pz = stage_pitch(it.Lz, true);  // staged row pitches
   const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + g * 32 + 2 * t;
-  const int ox = tl.p1_0 + g + a.colbase - it.colx;  // inside the staged x row for every lane
-  // z of planes outside the staged p3 range and y of combos outside the staged
-  // p2 range read column 0 instead (those combos' sums are never stored)
-  int oz[4];
+  // block n: x of plane p1_0[n] + g (inside the staged x row for every lane),
+  // z of plane p3_0[n] + g; z of planes outside the staged p3 range and y of
+  // combos outside the staged p2 range read column 0 instead (those combos'
+  // sums are never stored)
+  int ox[4], oz[4], oyb[4];
 #pragma unroll
   for (int n = 0; n < 4; ++n) {
-    const int o = tl.p3_0 + 8 * n + g + a.colbase - it.colz;
+    ox[n] = tl.p1_0[n] + g + a.colbase - it.colx;
+    const int o = tl.p3_0[n] + g + a.colbase - it.colz;
     oz[n] = (unsigned)o < (unsigned)it.Lz ? o : 0;
+    oyb[n] = -(tl.p1_0[n] + g) - (tl.p3_0[n] + 2 * t) + a.colbase - it.coly;  // y of (n, e): oyb[n] - e
   }
-  const int oyb = -(tl.p1_0 + g) - (tl.p3_0 + 2 * t) + a.colbase - it.coly;  // y of (n, e): oyb - 8n - e
   double sum[4][2];
 #pragma unroll
   for (int n = 0; n < 4; ++n) sum[n][0] = sum[n][1] = 0.0;
@@ -242,25 +245,24 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
       for (int k0 = 0; k0 < len; k0 += 4) {
         const bool on = k0 + t < len;
         const int row = tt + (on ? k0 + t : 0);
-        double2 xv = xs[row * px + ox];
-        if (!on) xv = make_double2(0.0, 0.0);
-        double2 zv[4];
+        double2 xv[4], zv[4];
 #pragma unroll
         for (int n = 0; n < 4; ++n) {
+          xv[n] = xs[row * px + ox[n]];
           zv[n] = zs[row * pz + oz[n]];
-          if (!on) zv[n] = make_double2(0.0, 0.0);
+          if (!on) xv[n] = zv[n] = make_double2(0.0, 0.0);
         }
         // first the products of the real parts of x, then those of the
         // imaginary parts: each accumulator's two MMAs are eight apart
 #pragma unroll
         for (int n = 0; n < 4; ++n) {
-          dmma884(wr[n][0], wr[n][1], xv.x, zv[n].x);
-          dmma884(wi[n][0], wi[n][1], xv.x, zv[n].y);
+          dmma884(wr[n][0], wr[n][1], xv[n].x, zv[n].x);
+          dmma884(wi[n][0], wi[n][1], xv[n].x, zv[n].y);
         }
 #pragma unroll
         for (int n = 0; n < 4; ++n) {
-          dmma884(wr[n][0], wr[n][1], -xv.y, zv[n].y);
-          dmma884(wi[n][0], wi[n][1], xv.y, zv[n].x);
+          dmma884(wr[n][0], wr[n][1], -xv[n].y, zv[n].y);
+          dmma884(wi[n][0], wi[n][1], xv[n].y, zv[n].x);
         }
       }
       tt += len;
@@ -269,7 +271,7 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
       for (int n = 0; n < 4; ++n)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          int o = oyb - 8 * n - e;
+          int o = oyb[n] - e;
           o = (unsigned)o < (unsigned)it.Ly ? o : 0;
           const double2 y = yr[o];
           sum[n][e] += fma(y.x, wr[n][e], -y.y * wi[n][e]);
