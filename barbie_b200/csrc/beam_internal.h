@@ -144,7 +144,11 @@ struct DevPlan {
   int32_t *bin_first = nullptr;   // [n_bins+1]
   double *ep_px = nullptr, *ep_pz = nullptr;  // [n_combo]
   int32_t *ep_cnt = nullptr;      // [n_combo] exact in-plane triangle count
+  int n_epchunks = 0;             // bins cut into chunks of at most EP_CHUNK triangles
+  int32_t *ep_chunk_first = nullptr;  // [n_epchunks+1] triangle ranges (bin order)
+  int32_t *bin_chunk = nullptr;   // [n_bins+1] chunk ranges per bin
 };
+constexpr int EP_CHUNK = 1024;  // most triangles per epilogue CTA
 
 // A stream plus the side streams the per-class triangle-sum launches fork onto.
 struct Lane {
@@ -171,6 +175,7 @@ struct RunSlot {
   double *B = nullptr;            // [cap][n_combo] triangle sums, bin order
   double *bins = nullptr;         // [cap][3][n_bins][16]: bs, norm, out
   long long *bin_count = nullptr; // [cap][n_bins]
+  double *ep_part = nullptr;      // [cap][n_epchunks][33] epilogue chunk sums
   int *status = nullptr;          // device status word
   double *h_staging = nullptr;    // pinned [cap][n_modes][Q]
   double *h_bins = nullptr;       // pinned [cap][3][n_bins][16]

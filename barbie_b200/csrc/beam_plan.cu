@@ -625,6 +625,21 @@ int build_plan_tables(beam_gpu_plan *p) {
   BEAM_TRY(upload(p, &d.u_nsplit, u_nsplit));
   BEAM_TRY(upload(p, &d.u_part, u_part));
   BEAM_TRY(upload(p, &d.bin_first, bin_first));
+  {
+    // epilogue chunks: each bin cut into ranges of at most EP_CHUNK triangles
+    std::vector<int32_t> chunk_first, bin_chunk(d.n_bins + 1, 0);
+    for (int b = 0; b < d.n_bins; ++b) {
+      bin_chunk[b] = (int32_t)chunk_first.size();
+      for (int32_t t = bin_first[b]; t < bin_first[b + 1]; t += EP_CHUNK) chunk_first.push_back(t);
+    }
+    bin_chunk[d.n_bins] = (int32_t)chunk_first.size();
+    d.n_epchunks = (int)chunk_first.size();
+    chunk_first.push_back(bin_first[d.n_bins]);
+    // chunk c covers [chunk_first[c], chunk_first[c+1]): bins are contiguous in
+    // bin order, so a bin's last chunk ends where the next non-empty bin begins
+    BEAM_TRY(upload(p, &d.ep_chunk_first, chunk_first));
+    BEAM_TRY(upload(p, &d.bin_chunk, bin_chunk));
+  }
   BEAM_TRY(upload(p, &d.ep_px, ep_px));
   BEAM_TRY(upload(p, &d.ep_pz, ep_pz));
   BEAM_TRY(upload(p, &d.ep_cnt, ep_cnt));
@@ -637,7 +652,8 @@ void free_plan_tables(beam_gpu_plan *p) {
   DevPlan &d = p->d;
   void *ptrs[] = {d.mode_ij,  d.mode_neg, d.ringmap, d.pixlocal,   d.tri_list, d.combo_u, d.combo_out,
                   d.u_cfirst, d.u_ncombo, d.u_nsplit, d.u_part,    d.tiles,    d.tile_combo, d.chunks,
-                  d.pieces,   d.descs,    d.items,    d.bin_first, d.ep_px,    d.ep_pz,   d.ep_cnt};
+                  d.pieces,   d.descs,    d.items,    d.bin_first, d.ep_px,    d.ep_pz,   d.ep_cnt,
+                  d.ep_chunk_first, d.bin_chunk};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   d = DevPlan();

@@ -108,63 +108,80 @@ __device__ __forceinline__ void orientation_weights(double px, double pz, double
 }
 
 constexpr int EP_THREADS = 128;
+constexpr int EP_VALS = 2 * BEAM_NPOLES + 1;  // bs[16], norm[16], count per chunk
 
-// One CTA per (k1, t, mu) bin (blockIdx.x) and realization (blockIdx.y) over
-// the bin's triangles (bin order = loop order within the bin). B == 0 drops the
-// triangle's count (barbie.c:355-357). Reduction order is fixed, so results are
-// run-to-run identical and do not depend on the batch a realization runs in.
-__global__ void __launch_bounds__(EP_THREADS) k_epilogue(const int32_t *__restrict__ bin_first,
-                                                         const double *__restrict__ B, long long b_stride,
-                                                         const double *__restrict__ px,
-                                                         const double *__restrict__ pz,
-                                                         const int32_t *__restrict__ cnt, double nn2, double vol,
-                                                         int n_bins, double *__restrict__ bins,
-                                                         long long *__restrict__ bin_count) {
-  __shared__ double red[2 * BEAM_NPOLES][EP_THREADS];
-  __shared__ long long redc[EP_THREADS];
-  const int b = blockIdx.x, tid = threadIdx.x;
+// Epilogue, pass 1: one CTA per chunk of at most EP_CHUNK triangles of one
+// (k1, t, mu) bin (blockIdx.x) and realization (blockIdx.y), in bin order
+// (loop order within the bin). Each triangle adds B * bs[ii] and Num * norm[ii]
+// with its cal_coeff weights; B == 0 drops the triangle's Num and count
+// (barbie.c:355-357). The CTA writes its chunk's 33 sums. Every reduction has a
+// fixed order, so results are run-to-run identical and do not depend on the
+// batch a realization runs in.
+__global__ void __launch_bounds__(EP_THREADS) k_ep_chunks(const int32_t *__restrict__ chunk_first, int n_chunks,
+                                                          const double *__restrict__ B, long long b_stride,
+                                                          const double *__restrict__ px,
+                                                          const double *__restrict__ pz,
+                                                          const int32_t *__restrict__ cnt, double nn2,
+                                                          double *__restrict__ part) {
+  __shared__ double red[EP_THREADS / 32][EP_VALS];
+  const int c = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   B += (size_t)blockIdx.y * b_stride;
-  bins += (size_t)blockIdx.y * 3 * n_bins * BEAM_NPOLES;
-  bin_count += (size_t)blockIdx.y * n_bins;
-  double sb[BEAM_NPOLES], sn[BEAM_NPOLES];
+  part += ((size_t)blockIdx.y * n_chunks + c) * EP_VALS;
+  double v[EP_VALS];
 #pragma unroll
-  for (int k = 0; k < BEAM_NPOLES; ++k) sb[k] = sn[k] = 0.0;
-  long long sc = 0;
-  for (int i = bin_first[b] + tid; i < bin_first[b + 1]; i += EP_THREADS) {
+  for (int k = 0; k < EP_VALS; ++k) v[k] = 0.0;
+  for (int i = chunk_first[c] + tid; i < chunk_first[c + 1]; i += EP_THREADS) {
     double Bv = B[i];
     double bs[BEAM_NPOLES], nm[BEAM_NPOLES];
     orientation_weights(px[i], pz[i], bs, nm);
     bool nz = (Bv != 0.0);
     double num = nz ? nn2 * (double)cnt[i] : 0.0;
-    sc += nz ? (long long)cnt[i] : 0;
+    v[2 * BEAM_NPOLES] += nz ? (double)cnt[i] : 0.0;
 #pragma unroll
     for (int k = 0; k < BEAM_NPOLES; ++k) {
-      sb[k] += Bv * bs[k];
-      sn[k] += num * nm[k];
+      v[k] += Bv * bs[k];
+      v[BEAM_NPOLES + k] += num * nm[k];
     }
   }
+  // fixed-order reduction: within each warp by halving, then warps in order
 #pragma unroll
-  for (int k = 0; k < BEAM_NPOLES; ++k) {
-    red[k][tid] = sb[k];
-    red[BEAM_NPOLES + k][tid] = sn[k];
-  }
-  redc[tid] = sc;
+  for (int k = 0; k < EP_VALS; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < EP_VALS; ++k) red[warp][k] = v[k];
   __syncthreads();
-  for (int s = EP_THREADS / 2; s > 0; s >>= 1) {
-    if (tid < s) {
+  if (tid < EP_VALS) {
+    double t = red[0][tid];
 #pragma unroll
-      for (int k = 0; k < 2 * BEAM_NPOLES; ++k) red[k][tid] += red[k][tid + s];
-      redc[tid] += redc[tid + s];
-    }
-    __syncthreads();
+    for (int w = 1; w < EP_THREADS / 32; ++w) t += red[w][tid];
+    part[tid] = t;
   }
-  if (tid < BEAM_NPOLES) {
-    double vbs = red[tid][0], vn = red[BEAM_NPOLES + tid][0];
-    bins[(size_t)b * BEAM_NPOLES + tid] = vbs;
-    bins[((size_t)n_bins + b) * BEAM_NPOLES + tid] = vn;
-    bins[((size_t)2 * n_bins + b) * BEAM_NPOLES + tid] = vbs / (vol * vn);
+}
+
+// Epilogue, pass 2: bin sums over the bin's chunks in order, the
+// normalisation out = bs / (vol * norm) (barbie.c:390) and the exact count.
+// One thread per (bin, pole); realization blockIdx.y.
+__global__ void k_ep_bins(const int32_t *__restrict__ bin_chunk, int n_bins, int n_chunks,
+                          const double *__restrict__ part, double vol, double *__restrict__ bins,
+                          long long *__restrict__ bin_count) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_bins * BEAM_NPOLES) return;
+  const int b = idx / BEAM_NPOLES, k = idx % BEAM_NPOLES;
+  part += (size_t)blockIdx.y * n_chunks * EP_VALS;
+  bins += (size_t)blockIdx.y * 3 * n_bins * BEAM_NPOLES;
+  bin_count += (size_t)blockIdx.y * n_bins;
+  double vbs = 0.0, vn = 0.0, vc = 0.0;
+  for (int c = bin_chunk[b]; c < bin_chunk[b + 1]; ++c) {
+    vbs += part[(size_t)c * EP_VALS + k];
+    vn += part[(size_t)c * EP_VALS + BEAM_NPOLES + k];
+    vc += part[(size_t)c * EP_VALS + 2 * BEAM_NPOLES];
   }
-  if (tid == 0) bin_count[b] = redc[0];
+  bins[(size_t)b * BEAM_NPOLES + k] = vbs;
+  bins[((size_t)n_bins + b) * BEAM_NPOLES + k] = vn;
+  bins[((size_t)2 * n_bins + b) * BEAM_NPOLES + k] = vbs / (vol * vn);
+  if (k == 0) bin_count[b] = (long long)vc;  // a sum of integers below 2^53: exact
 }
 
 // ------------------------------------------------------------ host drivers
@@ -195,7 +212,7 @@ void lane_destroy(Lane *l) {
 
 // Sizes of a slot's device buffers, in the order slot_alloc allocates them.
 struct SlotSizes {
-  size_t staging, src, S, part, B, bins, count;
+  size_t staging, src, S, part, B, bins, count, ep;
 };
 static SlotSizes slot_sizes(const beam_gpu_plan *p, int cap) {
   const DevPlan &d = p->d;
@@ -208,19 +225,20 @@ static SlotSizes slot_sizes(const beam_gpu_plan *p, int cap) {
   z.B = sizeof(double) * c * (size_t)std::max<long long>(1, d.n_combo);
   z.bins = sizeof(double) * c * 3 * (size_t)d.n_bins * BEAM_NPOLES;
   z.count = sizeof(long long) * c * (size_t)d.n_bins;
+  z.ep = sizeof(double) * c * (size_t)std::max(1, d.n_epchunks) * EP_VALS;
   return z;
 }
 
 size_t slot_bytes(const beam_gpu_plan *p, int cap) {
   SlotSizes z = slot_sizes(p, cap);
-  return z.staging + z.src + z.S + z.part + z.B + z.bins + z.count + sizeof(int);
+  return z.staging + z.src + z.S + z.part + z.B + z.bins + z.count + z.ep + sizeof(int);
 }
 
 void slot_destroy(RunSlot *s) {
   if (!s) return;
   if (s->lane && s->lane->stream) cudaStreamSynchronize(s->lane->stream);
   if (s->graph) cudaGraphExecDestroy(s->graph);
-  void *dev[] = {s->staging, (void *)s->src, s->S, s->part, s->B, s->bins, s->bin_count, s->status};
+  void *dev[] = {s->staging, (void *)s->src, s->S, s->part, s->B, s->bins, s->bin_count, s->ep_part, s->status};
   for (void *q : dev)
     if (q) cudaFree(q);
   void *host[] = {s->h_staging, (void *)s->h_src, s->h_bins, s->h_count, s->h_status};
@@ -244,6 +262,7 @@ static int slot_alloc(beam_gpu_plan *p, RunSlot *s) {
   BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->B, z.B));
   BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->bins, z.bins));
   BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->bin_count, z.count));
+  BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->ep_part, z.ep));
   BEAM_TRY(dev_alloc(&s->bytes, &s->status, 1));
   BEAM_CUDA(cudaMallocHost(&s->h_staging, std::max<size_t>(16, z.staging)));
   BEAM_CUDA(cudaMallocHost((void **)&s->h_src, z.src));
@@ -338,8 +357,16 @@ int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n) {
   if (d.n_bins == 0) return BEAM_OK;
   double nn2 = (double)p->geom.NN * (double)p->geom.NN;
   long long b_stride = std::max<long long>(1, d.n_combo);
-  k_epilogue<<<dim3((unsigned)d.n_bins, (unsigned)n), EP_THREADS, 0, s->lane->stream>>>(
-      d.bin_first, s->B, b_stride, d.ep_px, d.ep_pz, d.ep_cnt, nn2, p->geom.vol, d.n_bins, s->bins, s->bin_count);
+  cudaStream_t st = s->lane->stream;
+  if (d.n_epchunks > 0) {
+    k_ep_chunks<<<dim3((unsigned)d.n_epchunks, (unsigned)n), EP_THREADS, 0, st>>>(
+        d.ep_chunk_first, d.n_epchunks, s->B, b_stride, d.ep_px, d.ep_pz, d.ep_cnt, nn2, s->ep_part);
+    BEAM_CUDA(cudaGetLastError());
+    s->launches++;
+  }
+  const int threads = 256, cells = d.n_bins * BEAM_NPOLES;
+  k_ep_bins<<<dim3((unsigned)((cells + threads - 1) / threads), (unsigned)n), threads, 0, st>>>(
+      d.bin_chunk, d.n_bins, d.n_epchunks, s->ep_part, p->geom.vol, s->bins, s->bin_count);
   BEAM_CUDA(cudaGetLastError());
   s->launches++;
   return BEAM_OK;
