@@ -216,6 +216,17 @@ static void gather_one(const beam_gpu_plan *p, RunSlot *s, const double *r2c) {
   for (std::thread &t : th) t.join();
 }
 
+// Device-side address of a page-locked host buffer (cudaHostAlloc'd or
+// cudaHostRegister'ed), or nullptr for pageable memory.
+static const double *mapped_host(const double *r2c) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, r2c) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return at.type == cudaMemoryTypeHost ? static_cast<const double *>(at.devicePointer) : nullptr;
+}
+
 // Triangle sums of one realization on the plan's own slot.
 static int compute_B(beam_gpu_plan *p, const double *r2c, int on_device) {
   RunSlot *s = p->main;
@@ -226,6 +237,9 @@ static int compute_B(beam_gpu_plan *p, const double *r2c, int on_device) {
   if (on_device) {
     s->h_src[s->cap] = r2c;
     BEAM_TRY(upload_modes(p, s, 1, false));
+  } else if (const double *mapped = mapped_host(r2c)) {
+    BEAM_TRY(gather_mapped(p, s, mapped));
+    BEAM_TRY(upload_modes(p, s, 1, true, true));
   } else {
     gather_one(p, s, r2c);
     BEAM_TRY(upload_modes(p, s, 1, true));

@@ -235,7 +235,8 @@ int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out);
 void slot_destroy(RunSlot *s);
 // per-realization steps on a slot, for realizations [0, n) (beam_run.cu)
 void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c, int m0 = 0, int m1 = -1);
-int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged);
+int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged, bool staged_on_device = false);
+int gather_mapped(beam_gpu_plan *p, RunSlot *s, const double *r2c_mapped);
 int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n);
 int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n);
 int fetch_results(beam_gpu_plan *p, RunSlot *s, int n);

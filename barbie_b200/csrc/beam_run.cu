@@ -325,15 +325,38 @@ void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c, i
   }
 }
 
+// Realization 0's mode rows gathered by the device straight from a page-locked
+// host r2c buffer (r2c_mapped: its device-side address) into the slot's
+// staging rows: each needed row crosses the bus once, with no host-side gather.
+__global__ void k_gather_rows(const double2 *__restrict__ r2c_mapped, const int16_t *__restrict__ mode_ij,
+                              int n_modes, int Q, int NN, double2 *__restrict__ staging) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_modes * Q) return;
+  int m = (int)(idx / Q), q = (int)(idx % Q);
+  size_t row = ((size_t)mode_ij[2 * m] * NN + (size_t)mode_ij[2 * m + 1]) * (size_t)(NN / 2 + 1);
+  staging[idx] = r2c_mapped[row + q];
+}
+
+int gather_mapped(beam_gpu_plan *p, RunSlot *s, const double *r2c_mapped) {
+  const DevPlan &d = p->d;
+  long long n = (long long)d.n_modes * d.Q;
+  if (n == 0) return BEAM_OK;
+  k_gather_rows<<<(unsigned)((n + 255) / 256), 256, 0, s->lane->stream>>>(
+      (const double2 *)r2c_mapped, d.mode_ij, d.n_modes, d.Q, (int)p->geom.NN, (double2 *)s->staging);
+  BEAM_CUDA(cudaGetLastError());
+  s->launches++;
+  return BEAM_OK;
+}
+
 // Mode rows of realizations [0, n): from the pinned staging rows (staged) or
 // from the device r2c buffers the caller put in h_src[cap + r].
-int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged) {
+int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged, bool staged_on_device) {
   const DevPlan &d = p->d;
   cudaStream_t st = s->lane->stream;
-  if (staged) {
+  if (staged && !staged_on_device) {
     BEAM_CUDA(cudaMemcpyAsync(s->staging, s->h_staging, sizeof(double) * 2 * (size_t)n * d.n_modes * d.Q,
                               cudaMemcpyHostToDevice, st));
-  } else {
+  } else if (!staged) {
     BEAM_CUDA(cudaMemcpyAsync((void *)(s->src + s->cap), s->h_src + s->cap, sizeof(double *) * n,
                               cudaMemcpyHostToDevice, st));
   }

@@ -138,7 +138,11 @@ BEAM_API int beam_gpu_plan_get_info(const beam_gpu_plan *plan, beam_plan_info *i
  * (barbie.c:315-337), binning and cal_coeff weights (barbie.c:343-363,
  * funcs.c:708-745) and the normalisation (barbie.c:383-392).
  * r2c: double[NN][NN][NN+2], in host memory (r2c_on_device=0, pageable or
- * pinned) or device memory (r2c_on_device=1). Results go to host memory. */
+ * pinned) or device memory (r2c_on_device=1). Results go to host memory.
+ * Only the ring modes of the planes in use are read (6.6 MB of the 455 MB
+ * buffer at NN=384): from pageable memory the host gathers them and copies
+ * them over; from page-locked memory (cudaHostAlloc, cudaHostRegister) the
+ * device reads them in place. */
 BEAM_API int beam_gpu_run(beam_gpu_plan *plan, const double *r2c, int r2c_on_device, beam_result *res);
 
 /* Several realizations of one plan in one call (no counterpart in the
