@@ -57,7 +57,8 @@ class Cfg(ctypes.Structure):
 
 class Result(ctypes.Structure):
     _fields_ = [("bs", ctypes.POINTER(ctypes.c_double)), ("norm", ctypes.POINTER(ctypes.c_double)),
-                ("out", ctypes.POINTER(ctypes.c_double)), ("count", ctypes.POINTER(ctypes.c_int64))]
+                ("out", ctypes.POINTER(ctypes.c_double)), ("count", ctypes.POINTER(ctypes.c_int64)),
+                ("ana_sum", ctypes.POINTER(ctypes.c_double)), ("ana", ctypes.POINTER(ctypes.c_double))]
 
 
 class PlanInfo(ctypes.Structure):
@@ -129,6 +130,18 @@ def shard_assign(work, shard_count: int) -> np.ndarray:
     _check(L.beam_shard_assign(w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), w.size, shard_count,
                                owner.ctypes.data_as(ctypes.POINTER(ctypes.c_int))), "beam_shard_assign")
     return owner[: w.size]
+
+
+def _alloc_result(shape):
+    """A Result pointing at fresh numpy bin arrays of the given bin shape, and those arrays:
+    bs, norm, out, count, ana_sum (sum Biana*Num*bs) and ana (ana_sum/norm, column 5)."""
+    arrays = dict(bs=np.zeros(shape), norm=np.zeros(shape), out=np.zeros(shape),
+                  count=np.zeros(shape[:3], dtype=np.int64), ana_sum=np.zeros(shape), ana=np.zeros(shape))
+    dp = ctypes.POINTER(ctypes.c_double)
+    res = Result(arrays["bs"].ctypes.data_as(dp), arrays["norm"].ctypes.data_as(dp), arrays["out"].ctypes.data_as(dp),
+                 arrays["count"].ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), arrays["ana_sum"].ctypes.data_as(dp),
+                 arrays["ana"].ctypes.data_as(dp))
+    return res, arrays
 
 
 def _check(rc: int, what: str) -> None:
@@ -216,13 +229,7 @@ class Plan:
             pass
 
     def _result(self):
-        bs, nm, out = (np.zeros(self.shape) for _ in range(3))
-        cnt = np.zeros(self.shape[:3], dtype=np.int64)
-        res = Result(bs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                     nm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                     cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
-        return res, dict(bs=bs, norm=nm, out=out, count=cnt)
+        return _alloc_result(self.shape)
 
     def run(self, r2c) -> dict:
         """One bispectrum of an r2c buffer (numpy host array or torch CUDA tensor)."""
@@ -382,16 +389,11 @@ class Server:
         if info is None:
             raise BeamError(BEAM_EBUSY, "beam_gpu_server_take")
         shape = (info["n_k1bin"], info["n_mtbin"], info["n_mtbin"], NPOLES)
-        bs, nm, out = (np.zeros(shape) for _ in range(3))
-        cnt = np.zeros(shape[:3], dtype=np.int64)
-        res = Result(bs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                     nm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                     out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                     cnt.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        res, arrays = _alloc_result(shape)
         rc = _lib.beam_gpu_server_take(self._h, job, ctypes.byref(res))
         self._held.pop(job, None)
         _check(rc, "beam_gpu_server_take")
-        return dict(bs=bs, norm=nm, out=out, count=cnt, info=info)
+        return dict(arrays, info=info)
 
     def memory(self) -> tuple[int, int]:
         now, peak = ctypes.c_size_t(), ctypes.c_size_t()

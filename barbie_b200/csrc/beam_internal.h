@@ -143,12 +143,16 @@ struct DevPlan {
   int n_bins = 0;
   int32_t *bin_first = nullptr;   // [n_bins+1]
   double *ep_px = nullptr, *ep_pz = nullptr;  // [n_combo]
+  double *ep_ana = nullptr;       // [n_combo] analytic bispectrum of the triangle
   int32_t *ep_cnt = nullptr;      // [n_combo] exact in-plane triangle count
   int n_epchunks = 0;             // bins cut into chunks of at most EP_CHUNK triangles
   int32_t *ep_chunk_first = nullptr;  // [n_epchunks+1] triangle ranges (bin order)
   int32_t *bin_chunk = nullptr;   // [n_bins+1] chunk ranges per bin
 };
 constexpr int EP_CHUNK = 1024;  // most triangles per epilogue CTA
+// sections of a realization's bin array: sum B*bs, sum Num*norm, bs/(vol*norm),
+// sum Biana*Num*bs (each [n_bins][16])
+constexpr int BIN_SECTIONS = 4;
 
 // A stream plus the side streams the per-class triangle-sum launches fork onto.
 struct Lane {
@@ -173,12 +177,12 @@ struct RunSlot {
   void *S = nullptr;              // [cap][n_modes][W] complex mode data (double2 or float2)
   double *part = nullptr;         // [cap][n_part] partial sums (zero where never written)
   double *B = nullptr;            // [cap][n_combo] triangle sums, bin order
-  double *bins = nullptr;         // [cap][3][n_bins][16]: bs, norm, out
+  double *bins = nullptr;         // [cap][BIN_SECTIONS][n_bins][16]: bs, norm, out, analytic sum
   long long *bin_count = nullptr; // [cap][n_bins]
   double *ep_part = nullptr;      // [cap][n_epchunks][33] epilogue chunk sums
   int *status = nullptr;          // device status word
   double *h_staging = nullptr;    // pinned [cap][n_modes][Q]
-  double *h_bins = nullptr;       // pinned [cap][3][n_bins][16]
+  double *h_bins = nullptr;       // pinned [cap][BIN_SECTIONS][n_bins][16]
   long long *h_count = nullptr;   // pinned [cap][n_bins]
   int *h_status = nullptr;        // pinned status copy
   cudaEvent_t ev[5] = {};         // stage boundaries (beam_gpu_plan_last_timings)

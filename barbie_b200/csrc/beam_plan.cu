@@ -588,12 +588,13 @@ int build_plan_tables(beam_gpu_plan *p) {
                               &d.tri_list, &d.n_terms, &k2cnt));
 
   // epilogue tables in bin order
-  std::vector<double> ep_px(ntri), ep_pz(ntri);
+  std::vector<double> ep_px(ntri), ep_pz(ntri), ep_ana(ntri);
   std::vector<int32_t> ep_cnt(ntri);
   for (long long i = 0; i < ntri; ++i) {
     long long t = p->loop_of_bin[i];
     ep_px[i] = g.t_px[t];
     ep_pz[i] = g.t_pz[t];
+    ep_ana[i] = g.t_ana[t];
     int u = u_of_rp[g.t_rp[t]];
     ep_cnt[i] = (int32_t)(p->tri_first[u + 1] - p->tri_first[u]);
   }
@@ -642,6 +643,7 @@ int build_plan_tables(beam_gpu_plan *p) {
   }
   BEAM_TRY(upload(p, &d.ep_px, ep_px));
   BEAM_TRY(upload(p, &d.ep_pz, ep_pz));
+  BEAM_TRY(upload(p, &d.ep_ana, ep_ana));
   BEAM_TRY(upload(p, &d.ep_cnt, ep_cnt));
 
   d.elem = (p->cfg.precision == BEAM_PREC_MIXED) ? sizeof(float2) : sizeof(double2);
@@ -653,7 +655,7 @@ void free_plan_tables(beam_gpu_plan *p) {
   void *ptrs[] = {d.mode_ij,  d.mode_neg, d.ringmap, d.pixlocal,   d.tri_list, d.combo_u, d.combo_out,
                   d.u_cfirst, d.u_ncombo, d.u_nsplit, d.u_part,    d.tiles,    d.tile_combo, d.chunks,
                   d.pieces,   d.descs,    d.items,    d.bin_first, d.ep_px,    d.ep_pz,   d.ep_cnt,
-                  d.ep_chunk_first, d.bin_chunk};
+                  d.ep_chunk_first, d.bin_chunk, d.ep_ana};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   d = DevPlan();

@@ -108,19 +108,21 @@ __device__ __forceinline__ void orientation_weights(double px, double pz, double
 }
 
 constexpr int EP_THREADS = 128;
-constexpr int EP_VALS = 2 * BEAM_NPOLES + 1;  // bs[16], norm[16], count per chunk
+constexpr int EP_VALS = 3 * BEAM_NPOLES + 1;  // bs[16], norm[16], analytic[16], count per chunk
 
 // Epilogue, pass 1: one CTA per chunk of at most EP_CHUNK triangles of one
 // (k1, t, mu) bin (blockIdx.x) and realization (blockIdx.y), in bin order
-// (loop order within the bin). Each triangle adds B * bs[ii] and Num * norm[ii]
-// with its cal_coeff weights; B == 0 drops the triangle's Num and count
-// (barbie.c:355-357). The CTA writes its chunk's 33 sums. Every reduction has a
+// (loop order within the bin). Each triangle adds B * bs[ii], Num * norm[ii]
+// and Biana * Num * bs[ii] with its cal_coeff weights; B == 0 drops the
+// triangle's Num, Biana and count (barbie.c:355-361). The CTA writes its
+// chunk's EP_VALS sums. Every reduction has a
 // fixed order, so results are run-to-run identical and do not depend on the
 // batch a realization runs in.
 __global__ void __launch_bounds__(EP_THREADS) k_ep_chunks(const int32_t *__restrict__ chunk_first, int n_chunks,
                                                           const double *__restrict__ B, long long b_stride,
                                                           const double *__restrict__ px,
                                                           const double *__restrict__ pz,
+                                                          const double *__restrict__ ana,
                                                           const int32_t *__restrict__ cnt, double nn2,
                                                           double *__restrict__ part) {
   __shared__ double red[EP_THREADS / 32][EP_VALS];
@@ -136,11 +138,13 @@ __global__ void __launch_bounds__(EP_THREADS) k_ep_chunks(const int32_t *__restr
     orientation_weights(px[i], pz[i], bs, nm);
     bool nz = (Bv != 0.0);
     double num = nz ? nn2 * (double)cnt[i] : 0.0;
-    v[2 * BEAM_NPOLES] += nz ? (double)cnt[i] : 0.0;
+    double an = nz ? ana[i] : 0.0;
+    v[3 * BEAM_NPOLES] += nz ? (double)cnt[i] : 0.0;
 #pragma unroll
     for (int k = 0; k < BEAM_NPOLES; ++k) {
       v[k] += Bv * bs[k];
       v[BEAM_NPOLES + k] += num * nm[k];
+      v[2 * BEAM_NPOLES + k] += an * num * bs[k];
     }
   }
   // fixed-order reduction: within each warp by halving, then warps in order
@@ -161,7 +165,8 @@ __global__ void __launch_bounds__(EP_THREADS) k_ep_chunks(const int32_t *__restr
 }
 
 // Epilogue, pass 2: bin sums over the bin's chunks in order, the
-// normalisation out = bs / (vol * norm) (barbie.c:390) and the exact count.
+// normalisation out = bs / (vol * norm) (barbie.c:390), the analytic sum and
+// the exact count.
 // One thread per (bin, pole); realization blockIdx.y.
 __global__ void k_ep_bins(const int32_t *__restrict__ bin_chunk, int n_bins, int n_chunks,
                           const double *__restrict__ part, double vol, double *__restrict__ bins,
@@ -170,17 +175,19 @@ __global__ void k_ep_bins(const int32_t *__restrict__ bin_chunk, int n_bins, int
   if (idx >= n_bins * BEAM_NPOLES) return;
   const int b = idx / BEAM_NPOLES, k = idx % BEAM_NPOLES;
   part += (size_t)blockIdx.y * n_chunks * EP_VALS;
-  bins += (size_t)blockIdx.y * 3 * n_bins * BEAM_NPOLES;
+  bins += (size_t)blockIdx.y * BIN_SECTIONS * n_bins * BEAM_NPOLES;
   bin_count += (size_t)blockIdx.y * n_bins;
-  double vbs = 0.0, vn = 0.0, vc = 0.0;
+  double vbs = 0.0, vn = 0.0, va = 0.0, vc = 0.0;
   for (int c = bin_chunk[b]; c < bin_chunk[b + 1]; ++c) {
     vbs += part[(size_t)c * EP_VALS + k];
     vn += part[(size_t)c * EP_VALS + BEAM_NPOLES + k];
-    vc += part[(size_t)c * EP_VALS + 2 * BEAM_NPOLES];
+    va += part[(size_t)c * EP_VALS + 2 * BEAM_NPOLES + k];
+    vc += part[(size_t)c * EP_VALS + 3 * BEAM_NPOLES];
   }
   bins[(size_t)b * BEAM_NPOLES + k] = vbs;
   bins[((size_t)n_bins + b) * BEAM_NPOLES + k] = vn;
   bins[((size_t)2 * n_bins + b) * BEAM_NPOLES + k] = vbs / (vol * vn);
+  bins[((size_t)3 * n_bins + b) * BEAM_NPOLES + k] = va;
   if (k == 0) bin_count[b] = (long long)vc;  // a sum of integers below 2^53: exact
 }
 
@@ -223,7 +230,7 @@ static SlotSizes slot_sizes(const beam_gpu_plan *p, int cap) {
   z.S = d.elem * c * (size_t)d.n_modes * d.W;
   z.part = sizeof(double) * c * (size_t)d.n_part;
   z.B = sizeof(double) * c * (size_t)std::max<long long>(1, d.n_combo);
-  z.bins = sizeof(double) * c * 3 * (size_t)d.n_bins * BEAM_NPOLES;
+  z.bins = sizeof(double) * c * BIN_SECTIONS * (size_t)d.n_bins * BEAM_NPOLES;
   z.count = sizeof(long long) * c * (size_t)d.n_bins;
   z.ep = sizeof(double) * c * (size_t)std::max(1, d.n_epchunks) * EP_VALS;
   return z;
@@ -383,7 +390,7 @@ int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n) {
   cudaStream_t st = s->lane->stream;
   if (d.n_epchunks > 0) {
     k_ep_chunks<<<dim3((unsigned)d.n_epchunks, (unsigned)n), EP_THREADS, 0, st>>>(
-        d.ep_chunk_first, d.n_epchunks, s->B, b_stride, d.ep_px, d.ep_pz, d.ep_cnt, nn2, s->ep_part);
+        d.ep_chunk_first, d.n_epchunks, s->B, b_stride, d.ep_px, d.ep_pz, d.ep_ana, d.ep_cnt, nn2, s->ep_part);
     BEAM_CUDA(cudaGetLastError());
     s->launches++;
   }
@@ -402,7 +409,7 @@ int fetch_results(beam_gpu_plan *p, RunSlot *s, int n) {
   cudaStream_t st = s->lane->stream;
   size_t nb = (size_t)d.n_bins;
   if (nb) {
-    BEAM_CUDA(cudaMemcpyAsync(s->h_bins, s->bins, sizeof(double) * n * 3 * nb * BEAM_NPOLES, cudaMemcpyDeviceToHost,
+    BEAM_CUDA(cudaMemcpyAsync(s->h_bins, s->bins, sizeof(double) * n * BIN_SECTIONS * nb * BEAM_NPOLES, cudaMemcpyDeviceToHost,
                               st));
     BEAM_CUDA(cudaMemcpyAsync(s->h_count, s->bin_count, sizeof(long long) * n * nb, cudaMemcpyDeviceToHost, st));
   }
@@ -431,10 +438,13 @@ int check_status(RunSlot *s) {
 int copy_result(const beam_gpu_plan *p, const RunSlot *s, int r, beam_result *res) {
   if (!res) return BEAM_OK;
   size_t nb = (size_t)p->d.n_bins, n = nb * BEAM_NPOLES;
-  const double *h = s->h_bins + (size_t)r * 3 * n;
+  const double *h = s->h_bins + (size_t)r * BIN_SECTIONS * n;
   if (res->bs) std::memcpy(res->bs, h, sizeof(double) * n);
   if (res->norm) std::memcpy(res->norm, h + n, sizeof(double) * n);
   if (res->out) std::memcpy(res->out, h + 2 * n, sizeof(double) * n);
+  if (res->ana_sum) std::memcpy(res->ana_sum, h + 3 * n, sizeof(double) * n);
+  if (res->ana)
+    for (size_t i = 0; i < n; ++i) res->ana[i] = h[3 * n + i] / h[n + i];  // barbie.c:391
   if (res->count)
     for (size_t b = 0; b < nb; ++b) res->count[b] = (int64_t)s->h_count[(size_t)r * nb + b];
   return BEAM_OK;

@@ -78,7 +78,7 @@ struct Job {
   RunSlot *slot = nullptr;
   int n_k1bin = 0, n_mtbin = 0;
   long n_bins = 0;
-  std::vector<double> bins;  // [3][n_bins][16]
+  std::vector<double> bins;  // [BIN_SECTIONS][n_bins][16]
   std::vector<int64_t> count;
 };
 
@@ -252,7 +252,7 @@ bool retire(beam_gpu_server *s) {
     int rc = check_status(j->slot);
     if (rc == BEAM_OK) {
       size_t nb = (size_t)j->n_bins;
-      j->bins.assign(j->slot->h_bins, j->slot->h_bins + 3 * nb * BEAM_NPOLES);
+      j->bins.assign(j->slot->h_bins, j->slot->h_bins + BIN_SECTIONS * nb * BEAM_NPOLES);
       j->count.assign(j->slot->h_count, j->slot->h_count + nb);
       finish(s, j, BEAM_JOB_DONE, BEAM_OK, "");
     } else {
@@ -432,6 +432,9 @@ int beam_gpu_server_take(beam_gpu_server *s, int64_t job, beam_result *res) {
     if (res->bs) std::memcpy(res->bs, j->bins.data(), sizeof(double) * n);
     if (res->norm) std::memcpy(res->norm, j->bins.data() + n, sizeof(double) * n);
     if (res->out) std::memcpy(res->out, j->bins.data() + 2 * n, sizeof(double) * n);
+    if (res->ana_sum) std::memcpy(res->ana_sum, j->bins.data() + 3 * n, sizeof(double) * n);
+    if (res->ana)
+      for (size_t i = 0; i < n; ++i) res->ana[i] = j->bins[3 * n + i] / j->bins[n + i];  // barbie.c:391
     if (res->count) std::memcpy(res->count, j->count.data(), sizeof(int64_t) * (size_t)j->n_bins);
   }
   delete j;

@@ -33,7 +33,7 @@ int beam_ring_edges(long Nr, long Nmax, double *low, double *high, double *avg) 
 
 void beam_geom_free(beam_geom *g) {
   free(g->low); free(g->high); free(g->avg); free(g->ringmap); free(g->rp);
-  free(g->t_rp); free(g->t_p1); free(g->t_p2); free(g->t_bin); free(g->t_px); free(g->t_pz);
+  free(g->t_rp); free(g->t_p1); free(g->t_p2); free(g->t_bin); free(g->t_px); free(g->t_pz); free(g->t_ana);
   memset(g, 0, sizeof(*g));
 }
 
@@ -94,9 +94,16 @@ static int build_triplets(beam_geom *g) {
  * Returns 1 if the triangle passes |p3| < Nmax and LL_k1 < K1 < UL_k1. */
 typedef struct {
   double px, pz;
+  double ana;
   int bin;
   int bad_bin;
 } tri_eval;
+
+/* funcs.c:73-81: the input power spectrum P(k) = Av k^betav. */
+static double input_ps(double kk) {
+  double Av = 1.0, betav = -2.0;
+  return Av * pow(kk, betav);
+}
 
 static int eval_triangle(const beam_geom *g, int r1, int r2, int r3, int p1, int p2, tri_eval *e) {
   int p3 = -p1 - p2;
@@ -119,6 +126,15 @@ static int eval_triangle(const beam_geom *g, int r1, int r2, int r3, int p1, int
   double MU = 0.5 * (T + 1. / T - (k[2] / k[0]) * (k[2] / k[1]));
   e->pz = p[0] / k[0];
   e->px = ((p[1] / k[1]) + MU * e->pz) / (sqrt(1. - (MU * MU)));
+  /* barbie.c:300-305 with ff = 0.1, beta = 1 (barbie.c:79-80), Cunits of :77 */
+  {
+    const double ff = 0.1, beta = 1., Cunits = 2. * M_PI / (g->NN * g->LL);
+    double mu_1 = p[0] / k[0], mu_2 = p[1] / k[1], mu_3 = p[2] / k[2];
+    double ana = 2. * ff * (input_ps(Cunits * k[0]) * input_ps(Cunits * k[1]) +
+                            input_ps(Cunits * k[1]) * input_ps(Cunits * k[2]) +
+                            input_ps(Cunits * k[2]) * input_ps(Cunits * k[0]));
+    e->ana = ana * (1 + beta * mu_1 * mu_1) * (1 + beta * mu_2 * mu_2) * (1 + beta * mu_3 * mu_3);
+  }
   int n = g->n_mtbin;
   double kb = floor((K1 - (g->LL_k1)) / (1. * g->BW_k1));
   double tb = (T == 1) ? (n - 1) : floor((T - .5) / (.5 / (1. * n)));
@@ -173,6 +189,7 @@ static void enumerate_p1(enum_job *job, int p1) {
         g->t_bin[at] = e.bin;
         g->t_px[at] = e.px;
         g->t_pz[at] = e.pz;
+        g->t_ana[at] = e.ana;
         ++at;
       }
       ++n;
@@ -241,7 +258,8 @@ static int build_triangles(beam_geom *g) {
   g->t_bin = (int32_t *)malloc(sizeof(int32_t) * n);
   g->t_px = (double *)malloc(sizeof(double) * n);
   g->t_pz = (double *)malloc(sizeof(double) * n);
-  if (!g->t_rp || !g->t_p1 || !g->t_p2 || !g->t_bin || !g->t_px || !g->t_pz) {
+  g->t_ana = (double *)malloc(sizeof(double) * n);
+  if (!g->t_rp || !g->t_p1 || !g->t_p2 || !g->t_bin || !g->t_px || !g->t_pz || !g->t_ana) {
     rc = BEAM_ENOMEM;
   } else {
     job.fill = 1;

@@ -29,6 +29,7 @@ typedef struct beam_geom {
   int32_t *t_p1, *t_p2;     /* [ntri] planes of legs 1 and 2 (p3 = -p1-p2) */
   int32_t *t_bin;           /* [ntri] flattened (k1_bin, t_bin, mu_bin) */
   double *t_px, *t_pz;      /* [ntri] orientation parameters */
+  double *t_ana;            /* [ntri] analytic bispectrum of the triangle (barbie.c:300-305) */
   long iterations;          /* (p1, rp, p2) loop iterations visited */
 } beam_geom;
 

@@ -18,10 +18,11 @@
  *   BEAM_PRINT_DIGITS         significant digits of columns 4-6 (default: the
  *                             reference's %e / %f)
  * Differences from the reference, all on paths where it is undefined: the
- * analytic-comparison column 5 is written from a zero-initialised accumulator
- * (the reference never initialises bin_Biana, barbie.c:87,203-210), a missing
- * ResFiles_N<NN> directory is created, and invalid arguments or an unreadable
- * field file are reported instead of crashing. */
+ * analytic-comparison column 5 (the analytic bispectrum of P(k) = k^-2 over
+ * the bin's triangles, barbie.c:300-305,361,391) is accumulated from zero (the
+ * reference never initialises bin_Biana, barbie.c:87, and relies on zeroed
+ * stack pages), a missing ResFiles_N<NN> directory is created, and invalid
+ * arguments or an unreadable field file are reported instead of crashing. */
 #include <errno.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -109,12 +110,13 @@ int main(int argc, char *argv[]) {
   double *bs = (double *)calloc(nb * BEAM_NPOLES, sizeof(double));
   double *norm = (double *)calloc(nb * BEAM_NPOLES, sizeof(double));
   double *out = (double *)calloc(nb * BEAM_NPOLES, sizeof(double));
+  double *ana = (double *)calloc(nb * BEAM_NPOLES + 1, sizeof(double));
   int64_t *count = (int64_t *)calloc(nb ? nb : 1, sizeof(int64_t));
-  if (!bs || !norm || !out || !count) {
+  if (!bs || !norm || !out || !count || !ana) {
     fprintf(stderr, "barbie: out of host memory\n");
     return 1;
   }
-  beam_result res = {bs, norm, out, count};
+  beam_result res = {bs, norm, out, count, NULL, ana};
   double t1 = now_s();
   rc = beam_gpu_run(plan, field, 0, &res);
   if (rc) return fail("bispectrum", rc);
@@ -147,19 +149,19 @@ int main(int argc, char *argv[]) {
           size_t b = ((size_t)i * nm + j) * nm + l;
           double nrm = norm[b * BEAM_NPOLES + ii];
           double val = out[b * BEAM_NPOLES + ii];
-          double ana = 0.0 / nrm; /* zero-initialised analytic accumulator over its normalisation */
+          double an = ana[b * BEAM_NPOLES + ii]; /* bin_Biana / bin_normalization, barbie.c:391 */
           if (norm[b * BEAM_NPOLES + 0] > .1) {
             if (digits > 0)
-              fprintf(fp, "%d\t%d\t%d\t%.*e\t%.*e\t%.*e\n", i, j, l, digits - 1, val, digits - 1, ana, digits - 1,
+              fprintf(fp, "%d\t%d\t%d\t%.*e\t%.*e\t%.*e\n", i, j, l, digits - 1, val, digits - 1, an, digits - 1,
                       nrm / ((double)NN * NN * 1.));
             else
-              fprintf(fp, "%d\t%d\t%d\t%e\t%e\t%f\n", i, j, l, val, ana, nrm / ((double)NN * NN * 1.));
+              fprintf(fp, "%d\t%d\t%d\t%e\t%e\t%f\n", i, j, l, val, an, nrm / ((double)NN * NN * 1.));
           }
         }
     fclose(fp);
   }
   beam_gpu_plan_destroy(plan);
   beam_gpu_destroy(ctx);
-  free(field); free(bs); free(norm); free(out); free(count);
+  free(field); free(bs); free(norm); free(out); free(count); free(ana);
   return 0;
 }

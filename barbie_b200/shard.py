@@ -18,24 +18,30 @@ from __future__ import annotations
 import numpy as np
 
 
-def finalize(bs: np.ndarray, norm: np.ndarray, count: np.ndarray, vol: float) -> dict:
+def finalize(bs: np.ndarray, norm: np.ndarray, count: np.ndarray, vol: float, ana_sum=None) -> dict:
     """Bins from summed partials: out = bs / (vol * norm), as the epilogue
-    kernel and barbie.c:390 compute it (0/0 gives NaN for empty bins)."""
+    kernel and barbie.c:390 compute it, and ana = ana_sum / norm (barbie.c:391);
+    0/0 gives NaN for empty bins."""
+    if ana_sum is None:
+        ana_sum = np.zeros_like(bs)
     with np.errstate(divide="ignore", invalid="ignore"):
         out = bs / (vol * norm)
-    return dict(bs=bs, norm=norm, out=out, count=count)
+        ana = ana_sum / norm
+    return dict(bs=bs, norm=norm, out=out, count=count, ana_sum=ana_sum, ana=ana)
 
 
 def sum_partials(parts: list[dict], vol: float) -> dict:
     """Add the partial bins of all shards in shard order (one process)."""
     bs = np.zeros_like(parts[0]["bs"])
     norm = np.zeros_like(parts[0]["norm"])
+    ana_sum = np.zeros_like(parts[0]["bs"])
     count = np.zeros_like(parts[0]["count"])
     for p in parts:
         bs += p["bs"]
         norm += p["norm"]
+        ana_sum += p.get("ana_sum", 0.0)
         count += p["count"]
-    return finalize(bs, norm, count, vol)
+    return finalize(bs, norm, count, vol, ana_sum)
 
 
 def allreduce_partials(part: dict, vol: float, group=None, device=None) -> dict:
@@ -46,7 +52,8 @@ def allreduce_partials(part: dict, vol: float, group=None, device=None) -> dict:
     import torch.distributed as dist
 
     shape, cshape = part["bs"].shape, part["count"].shape
-    vals = torch.from_numpy(np.concatenate([part["bs"].ravel(), part["norm"].ravel()]))
+    ana_sum = part.get("ana_sum", np.zeros(shape))
+    vals = torch.from_numpy(np.concatenate([part["bs"].ravel(), part["norm"].ravel(), ana_sum.ravel()]))
     cnt = torch.from_numpy(np.ascontiguousarray(part["count"], dtype=np.int64).ravel().copy())
     if device is not None:
         vals, cnt = vals.to(device), cnt.to(device)
@@ -54,7 +61,8 @@ def allreduce_partials(part: dict, vol: float, group=None, device=None) -> dict:
     dist.all_reduce(cnt, op=dist.ReduceOp.SUM, group=group)
     vals, cnt = vals.cpu().numpy(), cnt.cpu().numpy()
     n = int(np.prod(shape))
-    return finalize(vals[:n].reshape(shape), vals[n:].reshape(shape), cnt.reshape(cshape), vol)
+    return finalize(vals[:n].reshape(shape), vals[n:2 * n].reshape(shape), cnt.reshape(cshape), vol,
+                    vals[2 * n:].reshape(shape))
 
 
 def run_sharded(ctx, r2c, rank: int, world: int, NN: int, UL_k1: int, LL_k1: int, BW_k1: int, *, group=None,

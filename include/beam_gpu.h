@@ -101,6 +101,9 @@ typedef struct beam_result {
   double *out;    /* bins: bs/(vol*norm)             (the value barbie.c:390-393 prints) */
   int64_t *count; /* [n_k1bin][n_mtbin][n_mtbin]: exact number of closed triangles summed
                      into the bin (those with B != 0); norm[..][0] = NN^2 * count */
+  double *ana_sum; /* bins: sum of Biana*Num*bs[ii], the analytic redshift-space bispectrum of
+                      P(k) = k^-2 over the bin's triangles (bin_Biana, barbie.c:300-305,361) */
+  double *ana;     /* bins: ana_sum/norm (column 5 of the output files, barbie.c:391-393) */
 } beam_result;
 
 typedef struct beam_plan_info {

@@ -259,6 +259,10 @@ long orc_enumerate(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1,
           t->rp = (int32_t)rp;
           t->K1 = K1; t->T = T; t->MU = MU; t->px = px; t->pz = pz;
           t->num = rings4[4 * rp + 3];
+          for (int i = 0; i < 3; ++i) {
+            t->leg_k[i] = K[i][0];
+            t->leg_p[i] = K[i][1];
+          }
           t->k1_bin = (int32_t)floor((K1 - (LL_k1)) / (1. * BW_k1));
           t->t_bin = shape_bin(T, n_mtbin);
           t->mu_bin = shape_bin(MU, n_mtbin);
@@ -284,9 +288,29 @@ double orc_triple_product(long NN, const double *F1, const double *F2, const dou
   return acc;
 }
 
+/* funcs.c:73-81 */
+static double input_ps(double kk) {
+  double Av = 1.0, betav = -2.0;
+  return Av * pow(kk, betav);
+}
+
+double orc_biana(long NN, double LL, const double leg_k[3], const double leg_p[3]) {
+  const double ff = 0.1, beta = 1.;           /* barbie.c:79-80 */
+  const double Cunits = 2. * M_PI / (NN * LL);  /* barbie.c:77 */
+  double mu_1 = leg_p[0] / leg_k[0], mu_2 = leg_p[1] / leg_k[1], mu_3 = leg_p[2] / leg_k[2];
+  double Biana = 2. * ff * (input_ps(Cunits * leg_k[0]) * input_ps(Cunits * leg_k[1]) +
+                            input_ps(Cunits * leg_k[1]) * input_ps(Cunits * leg_k[2]) +
+                            input_ps(Cunits * leg_k[2]) * input_ps(Cunits * leg_k[0]));
+  return Biana * (1 + beta * mu_1 * mu_1) * (1 + beta * mu_2 * mu_2) * (1 + beta * mu_3 * mu_3);
+}
+
+void orc_biana_all(long NN, double LL, const orc_triple *tri, long n, double *out) {
+  for (long t = 0; t < n; ++t) out[t] = orc_biana(NN, LL, tri[t].leg_k, tri[t].leg_p);
+}
+
 int orc_estimate(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1, int n_mtbin,
                  double LL, const double *r2c, double *bin_bs, double *bin_norm, double *bin_out,
-                 int64_t *counts, double *tri_B, long tri_cap, int nthreads) {
+                 int64_t *counts, double *tri_B, long tri_cap, int nthreads, double *bin_ana) {
   if (NN <= 0 || NN % 2 || Nmax <= 0 || Nmax > NN / 2 + 1 || BW_k1 <= 0 || UL_k1 <= LL_k1) return -1;
   double *low = (double *)calloc((size_t)Nr, sizeof(double));
   double *high = (double *)calloc((size_t)Nr, sizeof(double));
@@ -327,6 +351,7 @@ int orc_estimate(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1, i
   size_t nbins = (size_t)n_k1bin * n_mtbin * n_mtbin;
   memset(bin_bs, 0, sizeof(double) * nbins * ORC_NPOLES);
   memset(bin_norm, 0, sizeof(double) * nbins * ORC_NPOLES);
+  if (bin_ana) memset(bin_ana, 0, sizeof(double) * nbins * ORC_NPOLES);
   if (counts) memset(counts, 0, sizeof(int64_t) * nbins);
   int rc = 0;
   for (long t = 0; t < ntri; ++t) { /* barbie.c:343-363, in loop order */
@@ -339,10 +364,15 @@ int orc_estimate(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1, i
     double bs[ORC_NPOLES], nm[ORC_NPOLES];
     orc_cal_coeff(q->px, q->pz, bs, nm);
     double num = q->num;
-    if (B[t] == 0.) num = 0.; /* barbie.c:355-357 */
+    double ana = orc_biana(NN, LL, q->leg_k, q->leg_p);
+    if (B[t] == 0.) { /* barbie.c:355-357 */
+      ana = 0.;
+      num = 0.;
+    }
     size_t b = ((size_t)q->k1_bin * n_mtbin + q->t_bin) * n_mtbin + q->mu_bin;
     for (int ii = 0; ii < ORC_NPOLES; ++ii) {
       bin_bs[b * ORC_NPOLES + ii] += B[t] * bs[ii];
+      if (bin_ana) bin_ana[b * ORC_NPOLES + ii] += ana * num * bs[ii];
       bin_norm[b * ORC_NPOLES + ii] += num * nm[ii];
     }
     if (counts && B[t] != 0.) counts[b] += (int64_t)llround(q->num / (double)n2);

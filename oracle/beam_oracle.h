@@ -56,6 +56,7 @@ typedef struct {
   int32_t k1_bin, t_bin, mu_bin;  /* bins, barbie.c:343-345 */
   double K1, T, MU, px, pz;       /* shape parameters, barbie.c:293-297 */
   double num;                     /* rdata[rp][3], barbie.c:298 */
+  double leg_k[3], leg_p[3];      /* sorted legs K[i][0], K[i][1] (barbie.c:285-287) */
 } orc_triple;
 
 /* Enumerate the accepted triangles in the reference's loop order
@@ -75,11 +76,21 @@ long orc_enumerate(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1,
  * counts (optional, n_k1bin*n_mtbin*n_mtbin int64): sum over accepted
  * triangles with B != 0 of the exact integer triangle count round(Num/NN^2).
  * B per accepted triangle in enumeration order is written to tri_B if non-NULL.
+ * bin_ana (optional, same shape as bin_bs): sum of Biana*Num*bs, the analytic
+ * bispectrum accumulator of barbie.c:300-305,356-361 started from zero (the
+ * reference prints bin_ana/bin_norm as column 5, barbie.c:391-393).
  * nthreads > 1 splits the pixel sums over OpenMP threads.
  * Returns 0, or -1 on invalid arguments / allocation failure. */
 int orc_estimate(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1, int n_mtbin,
                  double LL, const double *r2c, double *bin_bs, double *bin_norm, double *bin_out,
-                 int64_t *counts, double *tri_B, long tri_cap, int nthreads);
+                 int64_t *counts, double *tri_B, long tri_cap, int nthreads, double *bin_ana);
+
+/* barbie.c:300-305: analytic redshift-space bispectrum of a triangle from its
+ * sorted legs (|K_i|, p_i) in grid units, cell size LL: P(k) = k^-2
+ * (input_ps, funcs.c:73-81), ff = 0.1, beta = 1 (barbie.c:79-80). */
+double orc_biana(long NN, double LL, const double leg_k[3], const double leg_p[3]);
+/* orc_biana of each of n enumerated triangles. */
+void orc_biana_all(long NN, double LL, const orc_triple *tri, long n, double *out);
 
 /* CPU-baseline timing on a bounded sample of one bispectrum's work: the
  * plane-ring transforms (Df) the sampled accepted triangles need and their

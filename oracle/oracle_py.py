@@ -33,6 +33,7 @@ class OrcTriple(ctypes.Structure):
         ("k1_bin", ctypes.c_int32), ("t_bin", ctypes.c_int32), ("mu_bin", ctypes.c_int32),
         ("K1", ctypes.c_double), ("T", ctypes.c_double), ("MU", ctypes.c_double),
         ("px", ctypes.c_double), ("pz", ctypes.c_double), ("num", ctypes.c_double),
+        ("leg_k", ctypes.c_double * 3), ("leg_p", ctypes.c_double * 3),
     ]
 
 
@@ -40,6 +41,7 @@ TRIPLE_DTYPE = np.dtype([
     ("p1", "<i4"), ("r1", "<i4"), ("p2", "<i4"), ("r2", "<i4"), ("p3", "<i4"), ("r3", "<i4"),
     ("rp", "<i4"), ("k1_bin", "<i4"), ("t_bin", "<i4"), ("mu_bin", "<i4"),
     ("K1", "<f8"), ("T", "<f8"), ("MU", "<f8"), ("px", "<f8"), ("pz", "<f8"), ("num", "<f8"),
+    ("leg_k", "<f8", (3,)), ("leg_p", "<f8", (3,)),
 ])
 assert TRIPLE_DTYPE.itemsize == ctypes.sizeof(OrcTriple)
 
@@ -71,8 +73,12 @@ def lib() -> ctypes.CDLL:
         L.orc_enumerate.restype = ctypes.c_long
         L.orc_estimate.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp, dp,
-                                   ctypes.POINTER(ctypes.c_int64), dp, ctypes.c_long, ctypes.c_int]
+                                   ctypes.POINTER(ctypes.c_int64), dp, ctypes.c_long, ctypes.c_int, dp]
         L.orc_estimate.restype = ctypes.c_int
+        L.orc_biana.argtypes = [ctypes.c_long, ctypes.c_double, dp, dp]
+        L.orc_biana.restype = ctypes.c_double
+        L.orc_biana_all.argtypes = [ctypes.c_long, ctypes.c_double, ctypes.c_void_p, ctypes.c_long, dp]
+        L.orc_biana_all.restype = None
         L.orc_triple_product.argtypes = [ctypes.c_long, dp, dp, dp, ctypes.c_int, ctypes.c_int]
         L.orc_triple_product.restype = ctypes.c_double
         L.orc_fft2d.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_int, dp]
@@ -145,15 +151,23 @@ def enumerate_triples(NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin=5, rings4=None)
     return out, int(iters.value)
 
 
+def biana(tri: np.ndarray, NN: int, LL: float = 1.0) -> np.ndarray:
+    """barbie.c:300-305: analytic bispectrum of each enumerated triangle."""
+    tri = np.ascontiguousarray(tri, dtype=TRIPLE_DTYPE)
+    out = np.zeros(max(1, len(tri)))
+    lib().orc_biana_all(NN, LL, tri.ctypes.data_as(ctypes.c_void_p), len(tri), _dp(out))
+    return out[: len(tri)]
+
+
 def estimate(r2c: np.ndarray, NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin=5, LL=1.0,
              nthreads=None, want_B=False):
     """The full estimator (barbie.c:110-397) with the plane-ring cache in RAM.
 
-    Returns dict(bs, norm, out, counts[, B]) with bins shaped
+    Returns dict(bs, norm, out, counts, ana, ana_out[, B]) with bins shaped
     [n_k1bin][n_mtbin][n_mtbin][16] (counts without the pole axis)."""
     n_k1bin = int((UL_k1 - LL_k1) / (1.0 * BW_k1))
     shape = (n_k1bin, n_mtbin, n_mtbin, NPOLES)
-    bs, nm, out = np.zeros(shape), np.zeros(shape), np.zeros(shape)
+    bs, nm, out, ana = np.zeros(shape), np.zeros(shape), np.zeros(shape), np.zeros(shape)
     counts = np.zeros(shape[:3], dtype=np.int64)
     ntri = 0
     B = None
@@ -164,10 +178,12 @@ def estimate(r2c: np.ndarray, NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin=5, LL=1
     rc = lib().orc_estimate(NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin, LL,
                             _dp(np.ascontiguousarray(r2c, dtype=np.float64)), _dp(bs), _dp(nm), _dp(out),
                             counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
-                            _dp(B) if B is not None else None, ntri, nthreads)
+                            _dp(B) if B is not None else None, ntri, nthreads, _dp(ana))
     if rc != 0:
         raise RuntimeError(f"orc_estimate failed ({rc})")
-    res = dict(bs=bs, norm=nm, out=out, counts=counts)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ana_out = ana / nm  # column 5 of the output files, barbie.c:391
+    res = dict(bs=bs, norm=nm, out=out, counts=counts, ana=ana, ana_out=ana_out)
     if want_B:
         res["B"] = B[:ntri]
     return res

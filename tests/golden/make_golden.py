@@ -6,12 +6,14 @@ compiled by oracle/Makefile from the reference's own barbie.c/funcs.c with the
 FFTW-API shim, printing %.17e instead of %e/%f -- in a scratch directory, and
 stores its 16 output files as one small .npz:
 
-  rows   float64[n, 6]: ii, k1 bin, t bin, mu bin, multipole value (column 4),
-         normalisation / NN^2 (column 6)
+  rows   float64[n, 7]: ii, k1 bin, t bin, mu bin, multipole value (column 4),
+         normalisation / NN^2 (column 6), analytic bispectrum (column 5)
   field_sha256, and the configuration.
 
-Column 5 (the analytic accumulator) is not stored: the reference never
-initialises it (barbie.c:87,203-210).
+Column 5 accumulates the analytic bispectrum (barbie.c:300-305,361,391) in an
+array the reference never initialises (barbie.c:87); in a fresh process the
+stack pages under it are zero, so its values are reproducible run to run, and
+the oracle's zero-initialised restatement is checked against them.
 
 Usage: python tests/golden/make_golden.py [case ...]     (default: all cases)
 Needs the reference sources (to build oracle/_ref) -- run where they exist.
@@ -67,7 +69,7 @@ def run_case(name: str, scratch: str) -> str:
         with open(path) as fh:
             for line in fh:
                 f = line.split()
-                rows.append([ii, int(f[0]), int(f[1]), int(f[2]), float(f[3]), float(f[5])])
+                rows.append([ii, int(f[0]), int(f[1]), int(f[2]), float(f[3]), float(f[5]), float(f[4])])
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(out, rows=np.array(rows, dtype=np.float64),
                         field_sha256=hashlib.sha256(field.tobytes()).hexdigest(),

@@ -19,7 +19,7 @@ class Geom(ctypes.Structure):
                 ("t_p1", ctypes.POINTER(ctypes.c_int32)), ("t_p2", ctypes.POINTER(ctypes.c_int32)),
                 ("t_bin", ctypes.POINTER(ctypes.c_int32)),
                 ("t_px", ctypes.POINTER(ctypes.c_double)), ("t_pz", ctypes.POINTER(ctypes.c_double)),
-                ("iterations", ctypes.c_long)]
+                ("t_ana", ctypes.POINTER(ctypes.c_double)), ("iterations", ctypes.c_long)]
 
 
 def build_geom(beamlib, NN, Nmax, Nr, UL, LL, BW, n_mtbin=5):
@@ -74,6 +74,9 @@ def test_geometry_bit_identical_to_oracle(beamlib, oracle, NN, Nmax, Nr, UL, LL,
         # bit-identical orientation parameters
         assert np.array_equal(arr(g.t_px, g.ntri, np.float64).view(np.int64), tri["px"].view(np.int64))
         assert np.array_equal(arr(g.t_pz, g.ntri, np.float64).view(np.int64), tri["pz"].view(np.int64))
+        # bit-identical analytic bispectrum per triangle (barbie.c:300-305)
+        ana = oracle.biana(tri, NN)
+        assert np.array_equal(arr(g.t_ana, g.ntri, np.float64).view(np.int64), ana.view(np.int64))
         assert g.vol == float(NN) ** 3
     finally:
         L.beam_geom_free(ctypes.byref(g))

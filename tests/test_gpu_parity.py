@@ -33,7 +33,7 @@ def test_fp64_matches_reference_outputs(beamlib, ctx, name):
     plan = make_plan(beamlib, ctx, name)
     res = plan.run(golden_field(name))
     NN = GOLDEN_CASES[name][0]
-    worst = compare_to_golden(g["rows"], res["out"], res["norm"], NN, rtol=1e-10)
+    worst = compare_to_golden(g["rows"], res["out"], res["norm"], NN, rtol=1e-10, ana=res["ana"])
     for r in g["rows"][g["rows"][:, 0] == 0]:
         assert res["count"][int(r[1]), int(r[2]), int(r[3])] == int(np.rint(r[5]))
     assert np.array_equal(res["norm"][..., 0], res["count"] * float(NN * NN))
@@ -48,10 +48,10 @@ def test_fp64_matches_oracle_arrays_and_triangle_sums(beamlib, ctx, oracle, name
     plan = make_plan(beamlib, ctx, name)
     res = plan.run(f)
     ok = want["norm"][..., 0] > 0.1
-    for key in ("bs", "norm"):
-        a, b = res[key][ok], want[key][ok]
+    for key, wkey in (("bs", "bs"), ("norm", "norm"), ("ana_sum", "ana")):
+        a, b = res[key][ok], want[wkey][ok]
         fin = np.isfinite(b)
-        assert np.all(np.abs(a[fin] - b[fin]) <= 1e-10 * np.abs(b[fin]) + 1e-300)
+        assert np.all(np.abs(a[fin] - b[fin]) <= 1e-10 * np.abs(b[fin]) + 1e-300), key
     assert np.array_equal(res["count"], want["counts"])
     B = plan.triangle_sums(f)
     Bo = want["B"]
@@ -181,7 +181,7 @@ def test_host_drop_in_cli(tmp_path):
     for ii in range(16):
         for line in open(tmp_path / f"ResFiles_N{NN}" / f"BS_test_ii{ii}_N{NN}_R{r}.txt"):
             f = line.split()
-            rows.append((ii, int(f[0]), int(f[1]), int(f[2]), float(f[3]), float(f[5])))
+            rows.append((ii, int(f[0]), int(f[1]), int(f[2]), float(f[3]), float(f[5]), float(f[4])))
     assert len(rows) == len(g["rows"])
     for mine, ref in zip(rows, g["rows"]):
         assert mine[:4] == tuple(int(v) for v in ref[:4])
@@ -190,3 +190,7 @@ def test_host_drop_in_cli(tmp_path):
         else:
             assert abs(mine[4] - ref[4]) <= 6e-7 * abs(ref[4])  # %e keeps 7 significant digits
         assert abs(mine[5] - ref[5]) <= 1e-6 * max(1, abs(ref[5]))
+        if np.isnan(ref[6]):  # column 5, the analytic bispectrum
+            assert np.isnan(mine[6])
+        else:
+            assert abs(mine[6] - ref[6]) <= 6e-7 * abs(ref[6])
