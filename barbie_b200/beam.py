@@ -306,6 +306,26 @@ class Plan:
             raise ValueError(f"r2c buffer must be [{NN}][{NN}][{NN + 2}] float64")
 
 
+PK_COLUMNS = ("k", "P0", "P2", "P4", "P6", "count")
+
+
+def power_multipoles(ctx: "Context", r2c, NN: int, LL: float = 0.56, Nbin: int = 10) -> dict:
+    """Power spectrum multipoles of an r2c buffer (beam_gpu_power_multipoles, the
+    reference's calpow_mom): arrays k, P0, P2, P4, P6, count over Nbin log bins."""
+    L = load()
+    L.beam_gpu_power_multipoles.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_double, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.beam_gpu_power_multipoles.restype = ctypes.c_int
+    addr, dev = _ptr(r2c)
+    if tuple(r2c.shape) not in ((NN, NN, NN + 2), (NN * NN * (NN + 2),)):
+        raise ValueError(f"r2c buffer must be [{NN}][{NN}][{NN + 2}] float64")
+    out = np.zeros(6 * Nbin)
+    _check(L.beam_gpu_power_multipoles(ctx._h, NN, LL, Nbin, addr, dev,
+                                       out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+           "beam_gpu_power_multipoles")
+    return dict(zip(PK_COLUMNS, out.reshape(6, Nbin)))
+
+
 class ServerCfg(ctypes.Structure):
     _fields_ = [("mem_budget", ctypes.c_size_t), ("max_active", ctypes.c_int), ("max_plans", ctypes.c_int)]
 

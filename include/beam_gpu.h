@@ -272,6 +272,17 @@ BEAM_API int beam_gpu_server_take(beam_gpu_server *srv, int64_t job, beam_result
 /* Device bytes the server holds now (cached plans + job buffers) and at most so far. */
 BEAM_API int beam_gpu_server_memory(const beam_gpu_server *srv, size_t *now, size_t *peak);
 
+/* Power spectrum multipoles of an r2c buffer: the reference's calpow_mom
+ * (funcs.c:860-1074, driven by calpow_mom.c). Every independent Fourier mode
+ * is binned in Nbin logarithmic bins of |k| (bin d holds log10(|k| NN) in
+ * [d, d+1) x log10(NN/2)/Nbin); out receives [6][Nbin] doubles: mean |k|
+ * (2 pi/(NN LL) units as the reference), P0, P2, P4, P6 and the mode count,
+ * normalised as funcs.c:1050-1066 with cell size LL (calpow_mom.c uses 0.56,
+ * Nbin 10). r2c in host (r2c_on_device=0) or device memory. Reads the whole
+ * buffer once on the context's stream. */
+BEAM_API int beam_gpu_power_multipoles(beam_gpu_ctx *ctx, long NN, double LL, int Nbin, const double *r2c,
+                                       int r2c_on_device, double *out);
+
 /* Human-readable text for an error code. */
 BEAM_API const char *beam_gpu_strerror(int code);
 

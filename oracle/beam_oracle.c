@@ -451,3 +451,80 @@ int orc_time_sample(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1
   free(low); free(high); free(avg); free(rings4); free(tri); free(RR); free(slot); free(slot_pr); free(F);
   return 0;
 }
+
+/* funcs.c:860-1074 (calpow_mom): power spectrum multipoles of the r2c buffer in
+ * Nbin logarithmic bins of |k|, with the reference's float/double types so the
+ * bin of every mode and the Legendre weights round as there. The three loops
+ * (half lines, half planes, half cube) visit each independent mode once. out
+ * receives [6][Nbin]: kmode, P0, P2, P4, P6, mode count (normalised as
+ * funcs.c:1050-1066 with cell size LL). */
+static void orc_pk_add(double *acc, int Nbin, long NN, float fac1, float fac2, float fac3, float scale, long a,
+                       long b, long c, const double *z) {
+  float m, mu, P2, P4, P6;
+  m = sqrt(fac1 * a * a + fac2 * b * b + fac3 * c * c);
+  mu = (1.0 * c) / (NN * m);
+  P2 = 0.5 * (3. * mu * mu - 1.);
+  P4 = 0.125 * (35.0 * powf(mu, 4.0) - 30.0 * mu * mu + 3);
+  P6 = 0.0625 * (231.0 * powf(mu, 6.0) - 315.0 * powf(mu, 4.0) + 105.0 * mu * mu - 5);
+  long d = (int)floorf(log10(m * NN) / scale);
+  if (d < 0 || d >= Nbin) return;
+  double pw = (z[0] * z[0]) + (z[1] * z[1]);
+  double *q = acc + 9 * d;
+  q[0] += pw;
+  q[1] += (double)(pw * P2);
+  q[2] += (double)(pw * P4);
+  q[3] += (double)(pw * P6);
+  q[4] += (double)m;
+  q[5] += 1.0;
+  q[6] += (double)(P2 * P2);
+  q[7] += (double)(P4 * P4);
+  q[8] += (double)(P6 * P6);
+}
+
+int orc_power_multipoles(long NN, double LL, int Nbin, const double *r2c, double *out) {
+  if (NN <= 0 || NN % 2 || Nbin <= 0 || !r2c || !out) return -1;
+  const long N1 = NN, N2 = NN, N3 = NN, NH = N3 / 2 + 1;
+  double *acc = (double *)calloc((size_t)Nbin * 9, sizeof(double));
+  if (!acc) return -1;
+  float fac1 = 1. / (1. * N1 * N1), fac2 = 1. / (1. * N2 * N2), fac3 = 1. / (1. * N3 * N3);
+  float scale = log10(0.5 * N1) / Nbin;
+  const double *z = r2c;
+  for (long i = 1; i <= N1 / 2; i++) /* half lines */
+    for (long j = 0; j <= N2 / 2; j = j + N2 / 2)
+      for (long k = 0; k <= N3 / 2; k = k + N3 / 2)
+        orc_pk_add(acc, Nbin, NN, fac1, fac2, fac3, scale, i, j, k, z + 2 * ((i * N2 + j) * NH + k));
+  for (long i = 0; i < N1; i++) { /* half planes */
+    long a = (i > N1 / 2) ? N1 - i : i;
+    for (long j = 1; j < N2 / 2; j++)
+      for (long k = 0; k <= N3 / 2; k = k + N3 / 2)
+        orc_pk_add(acc, Nbin, NN, fac1, fac2, fac3, scale, a, j, k, z + 2 * ((i * N2 + j) * NH + k));
+  }
+  for (long i = 0; i < N1; i++) { /* half cube */
+    long a = (i > N1 / 2) ? N1 - i : i;
+    for (long j = 0; j < N2; j++) {
+      long b = (j > N2 / 2) ? N2 - j : j;
+      for (long k = 1; k < N3 / 2; k++)
+        orc_pk_add(acc, Nbin, NN, fac1, fac2, fac3, scale, a, b, k, z + 2 * ((i * N2 + j) * NH + k));
+    }
+  }
+  double norml = 1. / (1. * N1 * N2 * N3), pi = M_PI;
+  for (int d = 0; d < Nbin; d++) {
+    const double *q = acc + 9 * d;
+    double kmode = q[4], P0 = q[0], P2 = q[1], P4 = q[2], P6 = q[3];
+    if (q[5] > 0.0) {
+      P0 = norml * P0 / (1.0 * q[5] * pow(LL, 3.));
+      kmode = 2. * pi * kmode / (q[5] * LL);
+    }
+    if (q[6] > 0.0) P2 = norml * P2 / (1.0 * q[6] * pow(LL, 3.));
+    if (q[7] > 0.0) P4 = norml * P4 / (1.0 * q[7] * pow(LL, 3.));
+    if (q[8] > 0.0) P6 = norml * P6 / (1.0 * q[8] * pow(LL, 3.));
+    out[d] = kmode;
+    out[Nbin + d] = P0;
+    out[2 * Nbin + d] = P2;
+    out[3 * Nbin + d] = P4;
+    out[4 * Nbin + d] = P6;
+    out[5 * Nbin + d] = q[5];
+  }
+  free(acc);
+  return 0;
+}

@@ -106,6 +106,11 @@ int orc_time_sample(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1
  * arrays (stored for planes |p| >= 0) and the conjugation signs. */
 double orc_triple_product(long NN, const double *F1, const double *F2, const double *F3, int sign2, int sign3);
 
+/* funcs.c:860-1074 (calpow_mom): power spectrum multipoles P0, P2, P4, P6 of the
+ * r2c buffer in Nbin logarithmic |k| bins, cell size LL. out: [6][Nbin] =
+ * kmode, P0, P2, P4, P6, mode count (the columns of calpow_mom.c:115). */
+int orc_power_multipoles(long NN, double LL, int Nbin, const double *r2c, double *out);
+
 #ifdef __cplusplus
 }
 #endif

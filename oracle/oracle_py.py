@@ -151,6 +151,18 @@ def enumerate_triples(NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin=5, rings4=None)
     return out, int(iters.value)
 
 
+def power_multipoles(r2c: np.ndarray, NN: int, LL: float = 0.56, Nbin: int = 10) -> dict:
+    """funcs.c:860-1074 (calpow_mom) -> arrays k, P0, P2, P4, P6, count over Nbin bins."""
+    L = lib()
+    L.orc_power_multipoles.argtypes = [ctypes.c_long, ctypes.c_double, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.orc_power_multipoles.restype = ctypes.c_int
+    out = np.zeros(6 * Nbin)
+    if L.orc_power_multipoles(NN, LL, Nbin, _dp(np.ascontiguousarray(r2c, dtype=np.float64)), _dp(out)) != 0:
+        raise ValueError("orc_power_multipoles: invalid arguments")
+    return dict(zip(("k", "P0", "P2", "P4", "P6", "count"), out.reshape(6, Nbin)))
+
+
 def biana(tri: np.ndarray, NN: int, LL: float = 1.0) -> np.ndarray:
     """barbie.c:300-305: analytic bispectrum of each enumerated triangle."""
     tri = np.ascontiguousarray(tri, dtype=TRIPLE_DTYPE)

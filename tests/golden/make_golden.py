@@ -15,7 +15,12 @@ array the reference never initialises (barbie.c:87); in a fresh process the
 stack pages under it are zero, so its values are reproducible run to run, and
 the oracle's zero-initialised restatement is checked against them.
 
-Usage: python tests/golden/make_golden.py [case ...]     (default: all cases)
+pk_<case>.npz holds the reference's power-spectrum multipoles of the same field
+(calpow_mom.c with funcs.c:860-1074, built as oracle/_ref/calpow_ref, printing
+%.17e): pk float64[n, 6] = k, P0, P2, P4, P6, mode count of the printed bins.
+
+Usage: python tests/golden/make_golden.py [--pk] [case ...]   (default: all cases;
+--pk makes only the pk_<case>.npz files)
 Needs the reference sources (to build oracle/_ref) -- run where they exist.
 """
 from __future__ import annotations
@@ -37,6 +42,7 @@ sys.path.insert(0, ROOT)
 from barbie_b200.synth import realization_seed, synth_field, write_field  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "barbie_ref")
+PK_BIN = os.path.join(ROOT, "oracle", "_ref", "calpow_ref")
 
 # name: (NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, realization)
 CASES = {
@@ -79,16 +85,39 @@ def run_case(name: str, scratch: str) -> str:
     return out
 
 
+def run_pk_case(name: str, scratch: str) -> str:
+    NN, r = CASES[name][0], CASES[name][6]
+    work = os.path.join(scratch, "pk_" + name)
+    shutil.rmtree(work, ignore_errors=True)
+    os.makedirs(os.path.join(work, f"ResFiles_N{NN}", "data_files"))
+    field = synth_field(NN, realization_seed(r))
+    write_field(os.path.join(work, f"ResFiles_N{NN}", "data_files", f"field_N{NN}_R{r}.txt"), field)
+    with open(os.path.join(work, "run.log"), "w") as log:
+        subprocess.run([PK_BIN, str(NN), str(r)], cwd=work, stdout=log, stderr=subprocess.STDOUT, check=True)
+    pk = np.loadtxt(os.path.join(work, f"ResFiles_N{NN}", f"psoutN{NN}_R{r}.dat"), ndmin=2)
+    out = os.path.join(HERE, f"pk_{name}.npz")
+    np.savez_compressed(out, pk=pk, field_sha256=hashlib.sha256(field.tobytes()).hexdigest(),
+                        config=np.array([NN, r], dtype=np.int64))
+    shutil.rmtree(work, ignore_errors=True)
+    print(f"pk_{name}: {len(pk)} bins -> {out}")
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("cases", nargs="*", default=list(CASES))
+    ap.add_argument("--pk", action="store_true", help="only the power-spectrum multipole fixtures")
     ap.add_argument("--scratch", default=os.path.join(HERE, ".scratch"))
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
     if not os.path.exists(REF_BIN):
         sys.exit("oracle/_ref/barbie_ref is missing: the reference sources are needed to build it")
     for c in args.cases:
-        run_case(c, args.scratch)
+        if args.pk:
+            run_pk_case(c, args.scratch)
+        else:
+            run_case(c, args.scratch)
+            run_pk_case(c, args.scratch)
     shutil.rmtree(args.scratch, ignore_errors=True)
 
 

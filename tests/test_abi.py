@@ -90,3 +90,13 @@ def test_host_cli_usage_and_errors(tmp_path):
     (tmp_path / "field_N64_R1.txt").write_bytes(b"\0" * 80)
     r = subprocess.run([exe, "64", "1", "11", "1", "1"], capture_output=True, text=True, cwd=tmp_path)
     assert r.returncode == 1 and "expected" in r.stderr
+
+
+def test_calpow_cli_usage_and_errors(tmp_path):
+    exe = os.path.join(ROOT, "barbie_b200", "calpow_mom")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "barbie_b200")], check=True)
+    r = subprocess.run([exe, "64"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and r.stdout.startswith("Usage:")  # calpow_mom.c:44-46
+    r = subprocess.run([exe, "64", "1"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and "field_N64_R1.txt" in r.stderr

@@ -116,3 +116,26 @@ def test_oracle_matches_reference_outputs(oracle, name):
     rows0 = g["rows"][g["rows"][:, 0] == 0]
     for r in rows0:
         assert res["counts"][int(r[1]), int(r[2]), int(r[3])] == int(np.rint(r[5]))
+
+
+def load_pk(name):
+    import os
+    from conftest import GOLDEN
+    path = os.path.join(GOLDEN, f"pk_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"power-spectrum fixture {name} not generated")
+    return np.load(path)["pk"]
+
+
+@pytest.mark.parametrize("name", ["nn64_cfg1", "nn96_r20"])
+def test_oracle_power_multipoles_match_reference(oracle, name):
+    """The restatement of calpow_mom (funcs.c:860-1074) against the reference
+    program's own output on the same field: bit for bit (same libm, same float
+    and double types)."""
+    NN = GOLDEN_CASES[name][0]
+    ref = load_pk(name)
+    got = oracle.power_multipoles(golden_field(name), NN, LL=0.56, Nbin=10)
+    mine = np.stack([got[c] for c in ("k", "P0", "P2", "P4", "P6", "count")], axis=1)
+    mine = mine[mine[:, 5] > 0]
+    assert mine.shape == ref.shape
+    assert np.array_equal(mine, ref)
