@@ -326,6 +326,56 @@ def power_multipoles(ctx: "Context", r2c, NN: int, LL: float = 0.56, Nbin: int =
     return dict(zip(PK_COLUMNS, out.reshape(6, Nbin)))
 
 
+def field_seed(NRi: int) -> int:
+    """The reference generator's seed for realization NRi (generate_field.c:49)."""
+    return 100020 + 146 * NRi
+
+
+def _field_out(NN: int, out):
+    if out is None:
+        out = np.empty((NN, NN, NN + 2))
+    if tuple(out.shape) not in ((NN, NN, NN + 2), (NN * NN * (NN + 2),)):
+        raise ValueError(f"r2c buffer must be [{NN}][{NN}][{NN + 2}] float64")
+    return out
+
+
+def generate_field(ctx: "Context", NN: int, seed: int, LL: float = 0.56, ff: float = 0.5, beta: float = 1.0,
+                   out=None):
+    """The reference's field generator on the device (beam_gpu_field_generate).
+
+    Returns (r2c, sigma): r2c is ``out`` (a float64 numpy array or CUDA tensor of
+    shape [NN][NN][NN+2]) or a new numpy array; sigma the Gaussian image's rms.
+    A device ``out`` stays on the device, ready for Plan.run."""
+    L = load()
+    L.beam_gpu_field_generate.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_ulonglong, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_double)]
+    L.beam_gpu_field_generate.restype = ctypes.c_int
+    out = _field_out(NN, out)
+    addr, dev = _ptr(out)
+    sigma = ctypes.c_double()
+    _check(L.beam_gpu_field_generate(ctx._h, NN, seed, LL, ff, beta, addr, dev, ctypes.byref(sigma)),
+           "beam_gpu_field_generate")
+    return out, sigma.value
+
+
+def ingest_field(ctx: "Context", cube, LL: float = 0.56, beta: float = 1.0, out=None):
+    """A real-space cube [NN][NN][NN] (numpy or CUDA tensor, float64) to the r2c
+    buffer on the device (beam_gpu_field_ingest): x LL^3, 3D r2c, RSD(beta)."""
+    L = load()
+    L.beam_gpu_field_ingest.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    L.beam_gpu_field_ingest.restype = ctypes.c_int
+    NN = int(cube.shape[0])
+    if tuple(cube.shape) != (NN, NN, NN):
+        raise ValueError("cube must be [NN][NN][NN]")
+    src, src_dev = _ptr(cube)
+    out = _field_out(NN, out)
+    addr, dev = _ptr(out)
+    _check(L.beam_gpu_field_ingest(ctx._h, NN, LL, beta, src, src_dev, addr, dev), "beam_gpu_field_ingest")
+    return out
+
+
 class ServerCfg(ctypes.Structure):
     _fields_ = [("mem_budget", ctypes.c_size_t), ("max_active", ctypes.c_int), ("max_plans", ctypes.c_int)]
 

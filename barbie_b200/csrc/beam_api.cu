@@ -108,6 +108,7 @@ int beam_gpu_init(int device, beam_gpu_ctx **out) {
 void beam_gpu_destroy(beam_gpu_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  if (ctx->field_ws) cudaFree(ctx->field_ws);
   lane_destroy(&ctx->lane);
   delete ctx;
 }

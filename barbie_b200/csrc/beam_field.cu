@@ -1,0 +1,602 @@
+// Field ingestion on the device: the reference's field generator
+// (generate_field.c:78-88 with ngrf_2d_funcs.c:341-584,734-765) and its
+// real-space-to-r2c step, producing the r2c buffer double[NN][NN][NN+2] that
+// beam_gpu_run reads, without leaving HBM.
+//
+// 3D transforms. A 3D DFT of the padded r2c layout is three passes of batched
+// 1D transforms, one per axis, each reading and writing the buffer once:
+//   * rows (last axis, contiguous): r2c / c2r of M rows per CTA;
+//   * columns (axes 0 and 1, strided): M adjacent k-columns per CTA, so every
+//     global access is M consecutive complex values (128 B at M = 8).
+// A CTA stages its M lines in shared memory and runs a Stockham autosort FFT
+// (radix 4, 2 and 3 stages, N = 2^a 3^b) between two buffers, one butterfly
+// per thread per step, with the twiddle table exp(-2 pi i n / N) in shared
+// memory. The transforms are unnormalised, FFTW's convention.
+//
+// Fused element work (no extra passes):
+//   * Make_Image's division by vol on the load of the first backward pass;
+//   * the per-row sum of squares for Non_Gauss's variance on the store of the
+//     last backward pass (rows), reduced in a fixed order by k_field_var;
+//   * Non_Gauss (x += ff (x^2 - var)) and Get_Modes (x *= LL^3) on the load of
+//     the first forward pass (rows);
+//   * RSD's (1 + beta mu^2) on the store of the last forward pass (axis 0).
+//
+// Gaussian modes (Fill_Modes). One thread per group of draws of the
+// reference's fill order (points, lines, planes, cubes); the index of each
+// draw in that order is a closed form of the group, and draw n of the stream
+// is a counter-based normal deviate (Philox4x32-10 + Box-Muller), so the
+// modes are filled in parallel with the values the sequential order gives.
+//
+// The file is compiled without FMA contraction, so the amplitude, scaling and
+// RSD factors round as the reference's C expressions do.
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "beam_internal.h"
+
+namespace beam {
+
+constexpr int FFT_THREADS = 256;
+constexpr int FFT_MAX_STAGES = 12;
+constexpr long FIELD_MAX_N = 1024;
+constexpr long FFT_TILE = 3072;  // complex values of one staging buffer (lines x length)
+
+struct FftGeom {
+  int N;  // line length
+  int M;  // lines per CTA
+  int nst;
+  int R[FFT_MAX_STAGES];
+};
+
+// N = 2^a 3^b: radix-4 stages, one radix-2 stage for an odd power of two, then radix-3
+static bool fft_geom(long N, FftGeom *g) {
+  if (N < 2 || N > FIELD_MAX_N) return false;
+  g->N = (int)N;
+  g->M = 16;
+  while (g->M > 1 && N * g->M > FFT_TILE) g->M >>= 1;
+  g->nst = 0;
+  long n = N;
+  while (n % 4 == 0 && g->nst < FFT_MAX_STAGES) g->R[g->nst++] = 4, n /= 4;
+  while (n % 2 == 0 && g->nst < FFT_MAX_STAGES) g->R[g->nst++] = 2, n /= 2;
+  while (n % 3 == 0 && g->nst < FFT_MAX_STAGES) g->R[g->nst++] = 3, n /= 3;
+  return n == 1;
+}
+
+static size_t fft_smem(const FftGeom &g) { return sizeof(double2) * ((size_t)g.N + 2 * (size_t)g.N * g.M); }
+
+// ---------------------------------------------------------------------------
+// Counter-based normal deviates: draw n of the stream with seed s is
+// Philox4x32-10(counter (n lo, n hi, 0, 0), key (s lo, s hi)) -> (u1, u2) ->
+// sqrt(-2 ln u1) cos(2 pi u2), u1 in (0, 1] and u2 in [0, 1) from the two
+// 64-bit halves (53 bits each). Philox: Salmon et al., "Parallel random
+// numbers: as easy as 1, 2, 3", SC'11.
+__device__ __forceinline__ double field_normal(unsigned long long seed, unsigned long long n) {
+  unsigned c0 = (unsigned)n, c1 = (unsigned)(n >> 32), c2 = 0u, c3 = 0u;
+  unsigned k0 = (unsigned)seed, k1 = (unsigned)(seed >> 32);
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const unsigned long long p0 = 0xD2511F53ull * c0, p1 = 0xCD9E8D57ull * c2;
+    const unsigned n0 = (unsigned)(p1 >> 32) ^ c1 ^ k0, n1 = (unsigned)p1;
+    const unsigned n2 = (unsigned)(p0 >> 32) ^ c3 ^ k1, n3 = (unsigned)p0;
+    c0 = n0, c1 = n1, c2 = n2, c3 = n3;
+    if (r < 9) k0 += 0x9E3779B9u, k1 += 0xBB67AE85u;
+  }
+  const unsigned long long a = (((unsigned long long)c1 << 32) | c0) >> 11;
+  const unsigned long long b = (((unsigned long long)c3 << 32) | c2) >> 11;
+  const double u1 = (double)(a + 1) * 0x1.0p-53, u2 = (double)b * 0x1.0p-53;
+  return sqrt(-2.0 * log(u1)) * cos(2.0 * M_PI * u2);
+}
+
+// Pk (ngrf_2d_funcs.c:143-155) with p(k) = 1.0 * k^-2 (ngrf_2d_funcs.c:132-140)
+__device__ __forceinline__ double field_pk(double C, long i, long j, long k) {
+  const double kx = C * i, ky = C * j, kz = C * k;
+  const double kk = sqrt(kx * kx + ky * ky + kz * kz);
+  return 1.0 * pow(kk, -2.0);
+}
+
+// Fill_Modes (ngrf_2d_funcs.c:341-510). Groups g in the reference's order,
+// with hh = N/2 - 1 interior values per half axis:
+//   g = 0            the k = 0 mode (zero, no draw)
+//   g = 1..7         points (i, j, k) in {0, N/2}^3, one draw each (draw g-1)
+//   8 + [0, 12 hh)   lines: (i, j) in {0,1}^2 x 3 axes x hh, two draws each
+//   next 12 hh^2     planes: (i, m) in {0,1}^2 x 3 orientations x hh^2, two draws
+//   next hh^3        cubes: four modes, eight draws
+__global__ void k_field_fill(double2 *__restrict__ A, long N, unsigned long long seed, double volfac, double C) {
+  const long h = N / 2, NH = N / 2 + 1, hh = h - 1;
+  const long nL = 12 * hh, nP = 12 * hh * hh, nC = hh * hh * hh;
+  long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (g >= 8 + nL + nP + nC) return;
+  auto at = [&](long i, long j, long k) { return (i * N + j) * NH + k; };
+  auto put2 = [&](long x, double amp, unsigned long long n) {
+    const double re = amp * field_normal(seed, n), im = amp * field_normal(seed, n + 1);
+    A[x] = make_double2(re, im);
+    return make_double2(re, im);
+  };
+  if (g < 8) {
+    if (g == 0) {
+      A[0] = make_double2(0.0, 0.0);
+      return;
+    }
+    const long i = g >> 2, j = (g >> 1) & 1, k = g & 1;
+    const double amp = sqrt(volfac * field_pk(C, i * h, j * h, k * h));
+    A[at(i * h, j * h, k * h)] = make_double2(amp * field_normal(seed, g - 1), 0.0);
+    return;
+  }
+  g -= 8;
+  if (g < nL) {  // ngrf_2d_funcs.c:387-428
+    const long ij = g / (3 * hh), rem = g % (3 * hh), axis = rem / hh, k = rem % hh + 1;
+    const long i = ij >> 1, j = ij & 1;
+    const unsigned long long n = 7 + 2 * (unsigned long long)g;
+    if (axis == 0) {
+      const double2 v = put2(at(k, i * h, j * h), sqrt(volfac * field_pk(C, k, i * h, j * h)), n);
+      A[at(N - k, i * h, j * h)] = make_double2(v.x, -v.y);
+    } else if (axis == 1) {
+      const double2 v = put2(at(i * h, k, j * h), sqrt(volfac * field_pk(C, i * h, k, j * h)), n);
+      A[at(i * h, N - k, j * h)] = make_double2(v.x, -v.y);
+    } else {
+      put2(at(i * h, j * h, k), sqrt(volfac * field_pk(C, i * h, j * h, k)), n);
+    }
+    return;
+  }
+  g -= nL;
+  if (g < nP) {  // ngrf_2d_funcs.c:432-481
+    const long im = g / (3 * hh * hh), rem = g % (3 * hh * hh), orient = rem / (hh * hh), q = rem % (hh * hh);
+    const long i = im >> 1, m = im & 1, j = q / hh + 1, k = q % hh + 1;
+    const unsigned long long n = 7 + 24 * (unsigned long long)hh + 2 * (unsigned long long)g;
+    const long jj1 = m ? N - j : j;
+    if (orient == 0) {
+      put2(at(i * h, jj1, k), sqrt(volfac * field_pk(C, i * h, j, k)), n);
+    } else if (orient == 1) {
+      put2(at(jj1, i * h, k), sqrt(volfac * field_pk(C, j, i * h, k)), n);
+    } else {
+      const long jj2 = m ? j : N - j;
+      const double2 v = put2(at(jj1, k, i * h), sqrt(volfac * field_pk(C, j, k, i * h)), n);
+      A[at(jj2, N - k, i * h)] = make_double2(v.x, -v.y);
+    }
+    return;
+  }
+  g -= nP;  // cubes, ngrf_2d_funcs.c:483-505
+  const long i = g / (hh * hh) + 1, j = (g / hh) % hh + 1, k = g % hh + 1;
+  const unsigned long long n = 7 + 24 * (unsigned long long)hh + 24 * (unsigned long long)(hh * hh) +
+                               8 * (unsigned long long)g;
+  const double amp = sqrt(volfac * field_pk(C, i, j, k));
+  put2(at(i, j, k), amp, n);
+  put2(at(N - i, j, k), amp, n + 2);
+  put2(at(i, N - j, k), amp, n + 4);
+  put2(at(N - i, N - j, k), amp, n + 6);
+}
+
+// ---------------------------------------------------------------------------
+// Stockham FFT of the CTA's M lines, from b0 into the returned buffer.
+// Stage s of radix R (Ns = product of the earlier radices): butterfly j reads
+// positions j + r N/R, applies the twiddles exp(-+2 pi i r (j mod Ns)/(Ns R)),
+// and writes positions (j - j mod Ns) R + j mod Ns + r Ns.
+// ROWS: line m at b[m N + p] (rows of the last axis); else b[p M + m].
+template <bool FWD>
+__device__ __forceinline__ double2 twmul(double2 a, double2 w) {
+  const double wy = FWD ? w.y : -w.y;
+  return make_double2(a.x * w.x - a.y * wy, a.x * wy + a.y * w.x);
+}
+
+template <bool FWD, bool ROWS>
+__device__ double2 *fft_lines(double2 *b0, double2 *b1, const double2 *__restrict__ tw, const FftGeom &g) {
+  const int N = g.N, M = g.M;
+  int Ns = 1;
+  for (int s = 0; s < g.nst; ++s) {
+    const int R = g.R[s], NR = N / R, tstr = N / (Ns * R);
+    for (int b = threadIdx.x; b < M * NR; b += blockDim.x) {
+      int m, j;
+      if (ROWS) {
+        m = b / NR;
+        j = b - m * NR;
+      } else {
+        j = b / M;
+        m = b - j * M;
+      }
+      const int js = j % Ns, o = (j - js) * R + js;
+      auto at = [&](int p) { return ROWS ? m * N + p : p * M + m; };
+      if (R == 4) {
+        const double2 a0 = b0[at(j)];
+        const double2 a1 = twmul<FWD>(b0[at(j + NR)], tw[js * tstr]);
+        const double2 a2 = twmul<FWD>(b0[at(j + 2 * NR)], tw[2 * js * tstr]);
+        const double2 a3 = twmul<FWD>(b0[at(j + 3 * NR)], tw[3 * js * tstr]);
+        const double2 y0 = make_double2(a0.x + a2.x, a0.y + a2.y), y1 = make_double2(a0.x - a2.x, a0.y - a2.y);
+        const double2 y2 = make_double2(a1.x + a3.x, a1.y + a3.y), y3 = make_double2(a1.x - a3.x, a1.y - a3.y);
+        b1[at(o)] = make_double2(y0.x + y2.x, y0.y + y2.y);
+        b1[at(o + 2 * Ns)] = make_double2(y0.x - y2.x, y0.y - y2.y);
+        if (FWD) {  // y1 -+ i y3
+          b1[at(o + Ns)] = make_double2(y1.x + y3.y, y1.y - y3.x);
+          b1[at(o + 3 * Ns)] = make_double2(y1.x - y3.y, y1.y + y3.x);
+        } else {
+          b1[at(o + Ns)] = make_double2(y1.x - y3.y, y1.y + y3.x);
+          b1[at(o + 3 * Ns)] = make_double2(y1.x + y3.y, y1.y - y3.x);
+        }
+      } else if (R == 2) {
+        const double2 a0 = b0[at(j)];
+        const double2 a1 = twmul<FWD>(b0[at(j + NR)], tw[js * tstr]);
+        b1[at(o)] = make_double2(a0.x + a1.x, a0.y + a1.y);
+        b1[at(o + Ns)] = make_double2(a0.x - a1.x, a0.y - a1.y);
+      } else {  // R == 3
+        const double c = 0.86602540378443864676;  // sqrt(3)/2
+        const double2 a0 = b0[at(j)];
+        const double2 a1 = twmul<FWD>(b0[at(j + NR)], tw[js * tstr]);
+        const double2 a2 = twmul<FWD>(b0[at(j + 2 * NR)], tw[2 * js * tstr]);
+        const double2 t = make_double2(a1.x + a2.x, a1.y + a2.y), d = make_double2(a1.x - a2.x, a1.y - a2.y);
+        const double2 mm = make_double2(a0.x - 0.5 * t.x, a0.y - 0.5 * t.y);
+        b1[at(o)] = make_double2(a0.x + t.x, a0.y + t.y);
+        if (FWD) {  // mm -+ i c d
+          b1[at(o + Ns)] = make_double2(mm.x + c * d.y, mm.y - c * d.x);
+          b1[at(o + 2 * Ns)] = make_double2(mm.x - c * d.y, mm.y + c * d.x);
+        } else {
+          b1[at(o + Ns)] = make_double2(mm.x - c * d.y, mm.y + c * d.x);
+          b1[at(o + 2 * Ns)] = make_double2(mm.x + c * d.y, mm.y - c * d.x);
+        }
+      }
+    }
+    __syncthreads();
+    double2 *t = b0;
+    b0 = b1;
+    b1 = t;
+    Ns *= R;
+  }
+  return b0;
+}
+
+// Column pass over axis 0 or 1 of the half-complex array (complex strides):
+// CTA blockIdx.x = outer * ntile + tile covers k-columns [tile M, tile M + M).
+struct ColPass {
+  double2 *data;
+  long outer_stride, elem_stride;
+  int NH, ntile;
+  double in_div;  // > 0: loaded values are divided by it (Make_Image, ngrf_2d_funcs.c:521-527)
+  int rsd;        // axis-0 pass: RSD factor on the store (ngrf_2d_funcs.c:743-762)
+  double beta;
+};
+
+template <bool FWD>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_cols(ColPass a, FftGeom g, const double2 *__restrict__ twg) {
+  extern __shared__ double2 fsm[];
+  const int N = g.N, M = g.M;
+  double2 *tw = fsm, *b0 = fsm + N, *b1 = b0 + (size_t)N * M;
+  const long outer = blockIdx.x / a.ntile;
+  const int k0 = (int)(blockIdx.x % a.ntile) * M, mc = min(M, a.NH - k0);
+  double2 *base = a.data + outer * a.outer_stride + k0;
+  for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
+  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
+    const int p = e / M, m = e - p * M;
+    double2 v = make_double2(0.0, 0.0);
+    if (m < mc) {
+      v = base[p * a.elem_stride + m];
+      if (a.in_div > 0) v = make_double2(v.x / a.in_div, v.y / a.in_div);
+    }
+    b0[e] = v;
+  }
+  __syncthreads();
+  const double2 *r = fft_lines<FWD, false>(b0, b1, tw, g);
+  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
+    const int p = e / M, m = e - p * M;
+    if (m >= mc) continue;
+    double2 v = r[e];
+    if (a.rsd) {  // element (i, j, k) = (p, outer, k0 + m)
+      const long k = k0 + m;
+      const double ia = (p > N / 2) ? (N - p) : p, ja = (outer > N / 2) ? (N - outer) : outer;
+      const double kk = sqrt(1. * (ia * ia + ja * ja + (double)(k * k)));
+      if (p + outer + k != 0) {
+        const double myu = k / kk;
+        v.x *= (1. + a.beta * myu * myu);
+        v.y *= (1. + a.beta * myu * myu);
+      }
+    }
+    base[p * a.elem_stride + m] = v;
+  }
+}
+
+// Row pass over the last axis of the padded buffer (N+2 doubles per row).
+struct RowPass {
+  double *data;
+  const double *src;  // r2c: rows read from here (data, or a dense real cube)
+  long src_pitch;     // doubles
+  long nrows;
+  const double *var;  // r2c: Non_Gauss with this variance first (nullptr: none)
+  double ff, lcube;   // r2c: x += ff (x^2 - var); x *= lcube (ngrf_2d_funcs.c:540-546,580-582)
+  double *row_sumsq;  // c2r: per-row sum of x^2 of the output
+};
+
+// forward r2c of M rows: real row -> its N/2+1 complex values, in place
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_r2c(RowPass a, FftGeom g, const double2 *__restrict__ twg) {
+  extern __shared__ double2 fsm[];
+  const int N = g.N, M = g.M, NH = N / 2 + 1;
+  double2 *tw = fsm, *b0 = fsm + N, *b1 = b0 + (size_t)N * M;
+  const long r0 = (long)blockIdx.x * M;
+  for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
+  const double var = a.var ? *a.var : 0.0;
+  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
+    const int m = e / N, p = e - m * N;
+    const long row = r0 + m;
+    double x = 0.0;
+    if (row < a.nrows) {
+      x = a.src[row * a.src_pitch + p];
+      if (a.var) x += a.ff * (x * x - var);
+      x = x * a.lcube;
+    }
+    b0[e] = make_double2(x, 0.0);
+  }
+  __syncthreads();
+  const double2 *r = fft_lines<true, true>(b0, b1, tw, g);
+  double2 *out = (double2 *)a.data;
+  for (int e = threadIdx.x; e < NH * M; e += blockDim.x) {
+    const int m = e / NH, q = e - m * NH;
+    const long row = r0 + m;
+    if (row < a.nrows) out[row * NH + q] = r[m * N + q];
+  }
+}
+
+// backward c2r of M rows: N/2+1 complex values (Hermitian extension, the
+// imaginary parts of k = 0 and N/2 dropped) -> N real values, in place
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_c2r(RowPass a, FftGeom g, const double2 *__restrict__ twg) {
+  extern __shared__ double2 fsm[];
+  const int N = g.N, M = g.M, NH = N / 2 + 1;
+  double2 *tw = fsm, *b0 = fsm + N, *b1 = b0 + (size_t)N * M;
+  const long r0 = (long)blockIdx.x * M;
+  const double2 *in = (const double2 *)a.data;
+  for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
+  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
+    const int m = e / N, p = e - m * N;
+    const long row = r0 + m;
+    double2 v = make_double2(0.0, 0.0);
+    if (row < a.nrows) {
+      v = in[row * NH + (p <= N / 2 ? p : N - p)];
+      if (p > N / 2) v.y = -v.y;
+      if (p == 0 || p == N / 2) v.y = 0.0;
+    }
+    b0[e] = v;
+  }
+  __syncthreads();
+  const double2 *r = fft_lines<false, true>(b0, b1, tw, g);
+  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
+    const int m = e / N, p = e - m * N;
+    const long row = r0 + m;
+    if (row < a.nrows) a.data[row * (N + 2) + p] = r[e].x;
+  }
+  if (a.row_sumsq) {  // one warp per row, lanes in a fixed order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int m = warp; m < M; m += FFT_THREADS / 32) {
+      double s = 0.0;
+      for (int p = lane; p < N; p += 32) s += r[m * N + p].x * r[m * N + p].x;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0 && r0 + m < a.nrows) a.row_sumsq[r0 + m] = s;
+    }
+  }
+}
+
+// variance of the image (Non_Gauss, ngrf_2d_funcs.c:563-570): the row sums in
+// a fixed order, / (1. * N * N * N)
+__global__ void __launch_bounds__(1024) k_field_var(const double *__restrict__ row_sumsq, long nrows, long N,
+                                                    double *__restrict__ var) {
+  __shared__ double part[32];
+  double s = 0.0;
+  for (long r = threadIdx.x; r < nrows; r += blockDim.x) s += row_sumsq[r];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = part[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) *var = s / (1. * N * N * N);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+
+static bool field_size_ok(long N) {
+  if (N < 4 || N % 2 || N > FIELD_MAX_N) return false;
+  long n = N;
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  return n == 1;
+}
+
+// exp(-2 pi i n / N) rounded from long double
+static void twiddles(long N, std::vector<double2> &tw) {
+  tw.resize(N);
+  const long double pi = acosl(-1.0L);
+  for (long n = 0; n < N; ++n) {
+    const long double t = 2.0L * pi * (long double)n / (long double)N;
+    tw[n] = make_double2((double)cosl(t), (double)-sinl(t));
+  }
+}
+
+struct FieldRun {
+  beam_gpu_ctx *ctx;
+  long N;
+  FftGeom g;
+  double2 *tw = nullptr;        // device twiddle table
+  double *row_sumsq = nullptr;  // [N^2]
+  double *var = nullptr;
+  int launches = 0;
+};
+
+static int field_workspace(FieldRun &f) {
+  beam_gpu_ctx *c = f.ctx;
+  const size_t need = sizeof(double2) * f.N + sizeof(double) * (f.N * f.N + 2);
+  if (c->field_ws_bytes < need) {
+    if (c->field_ws) cudaFree(c->field_ws);
+    c->field_ws = nullptr;
+    c->field_ws_bytes = 0;
+    size_t got = 0;
+    int rc = dev_alloc(&got, (char **)&c->field_ws, need);
+    if (rc != BEAM_OK) return rc;
+    c->field_ws_bytes = need;
+  }
+  f.tw = (double2 *)c->field_ws;
+  f.var = (double *)(f.tw + f.N);
+  f.row_sumsq = f.var + 2;
+  std::vector<double2> tw;
+  twiddles(f.N, tw);
+  BEAM_CUDA(cudaMemcpyAsync(f.tw, tw.data(), sizeof(double2) * f.N, cudaMemcpyHostToDevice, c->stream));
+  // a synchronous host array: wait before it goes out of scope
+  BEAM_CUDA(cudaStreamSynchronize(c->stream));
+  const int smem = (int)fft_smem(f.g);
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_cols<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  return BEAM_OK;
+}
+
+// column passes: axis 0 (i; outer index j) or axis 1 (j; outer index i)
+template <bool FWD>
+static void launch_cols(FieldRun &f, double *buf, int axis, double in_div, int rsd, double beta) {
+  const long N = f.N, NH = N / 2 + 1;
+  ColPass a{};
+  a.data = (double2 *)buf;
+  a.outer_stride = axis == 0 ? NH : N * NH;
+  a.elem_stride = axis == 0 ? N * NH : NH;
+  a.NH = (int)NH;
+  a.ntile = (int)((NH + f.g.M - 1) / f.g.M);
+  a.in_div = in_div;
+  a.rsd = rsd;
+  a.beta = beta;
+  k_fft_cols<FWD><<<(unsigned)(N * a.ntile), FFT_THREADS, fft_smem(f.g), f.ctx->stream>>>(a, f.g, f.tw);
+  ++f.launches;
+}
+
+static void launch_rows_r2c(FieldRun &f, double *buf, const double *src, long src_pitch, bool nongauss, double ff,
+                            double lcube) {
+  RowPass a{};
+  a.data = buf;
+  a.src = src;
+  a.src_pitch = src_pitch;
+  a.nrows = f.N * f.N;
+  a.var = nongauss ? f.var : nullptr;
+  a.ff = ff;
+  a.lcube = lcube;
+  k_fft_rows_r2c<<<(unsigned)((a.nrows + f.g.M - 1) / f.g.M), FFT_THREADS, fft_smem(f.g), f.ctx->stream>>>(a, f.g,
+                                                                                                          f.tw);
+  ++f.launches;
+}
+
+static void launch_rows_c2r(FieldRun &f, double *buf) {
+  RowPass a{};
+  a.data = buf;
+  a.nrows = f.N * f.N;
+  a.row_sumsq = f.row_sumsq;
+  k_fft_rows_c2r<<<(unsigned)((a.nrows + f.g.M - 1) / f.g.M), FFT_THREADS, fft_smem(f.g), f.ctx->stream>>>(a, f.g,
+                                                                                                          f.tw);
+  ++f.launches;
+}
+
+static int field_begin(beam_gpu_ctx *ctx, long NN, double LL, FieldRun &f) {
+  if (!field_size_ok(NN) || !(LL > 0) || !std::isfinite(LL)) {
+    set_detail("field: NN must be 2^a 3^b, even, in [4, 1024], and LL > 0");
+    return BEAM_EINVAL;
+  }
+  f.ctx = ctx;
+  f.N = NN;
+  if (!fft_geom(NN, &f.g) || fft_smem(f.g) > ctx->smem_optin) {
+    set_detail("field: no FFT geometry for this NN");
+    return BEAM_EINVAL;
+  }
+  BEAM_CUDA(cudaSetDevice(ctx->device));
+  return field_workspace(f);
+}
+
+// the output buffer: the caller's device buffer, or a temporary one
+static int field_out(const FieldRun &f, double *r2c, int r2c_on_device, double **buf) {
+  if (r2c_on_device) {
+    *buf = r2c;
+    return BEAM_OK;
+  }
+  size_t got = 0;
+  return dev_alloc(&got, buf, (size_t)f.N * f.N * (f.N + 2));
+}
+
+static int field_end(FieldRun &f, double *buf, double *r2c, int r2c_on_device, double *var_out) {
+  cudaStream_t st = f.ctx->stream;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && !r2c_on_device)
+    e = cudaMemcpyAsync(r2c, buf, sizeof(double) * f.N * f.N * (f.N + 2), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && var_out) e = cudaMemcpyAsync(var_out, f.var, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (!r2c_on_device) cudaFree(buf);
+  if (e != cudaSuccess) {
+    set_detail(std::string("field: ") + cudaGetErrorString(e));
+    return BEAM_ECUDA;
+  }
+  f.ctx->field_launches = f.launches;
+  return BEAM_OK;
+}
+
+}  // namespace beam
+
+using namespace beam;
+
+extern "C" int beam_gpu_field_generate(beam_gpu_ctx *ctx, long NN, unsigned long long seed, double LL, double ff,
+                                       double beta, double *r2c, int r2c_on_device, double *sigma) {
+  if (!ctx || !r2c || !std::isfinite(ff) || !std::isfinite(beta)) {
+    set_detail("field generate: null context or buffer, or non-finite ff / beta");
+    return BEAM_EINVAL;
+  }
+  FieldRun f;
+  int rc = field_begin(ctx, NN, LL, f);
+  if (rc != BEAM_OK) return rc;
+  double *buf = nullptr;
+  if ((rc = field_out(f, r2c, r2c_on_device, &buf)) != BEAM_OK) return rc;
+  const long N = NN, h = N / 2, hh = h - 1;
+  // generate_field.c:54-56
+  const double vol = pow((N * LL), 3), C = 2. * M_PI / (N * LL);
+  const long groups = 8 + 12 * hh + 12 * hh * hh + hh * hh * hh;
+  k_field_fill<<<(unsigned)((groups + 255) / 256), 256, 0, ctx->stream>>>((double2 *)buf, N, seed, vol / 2., C);
+  ++f.launches;
+  // Make_Image: / vol, c2r (axis 0, axis 1, rows); the rows keep their sums of squares
+  launch_cols<false>(f, buf, 0, vol, 0, 0.0);
+  launch_cols<false>(f, buf, 1, 0.0, 0, 0.0);
+  launch_rows_c2r(f, buf);
+  // Non_Gauss's variance, then Non_Gauss + Get_Modes + r2c (rows, axis 1, axis 0 with RSD)
+  k_field_var<<<1, 1024, 0, ctx->stream>>>(f.row_sumsq, N * N, N, f.var);
+  ++f.launches;
+  launch_rows_r2c(f, buf, buf, N + 2, true, ff, pow(LL, 3.));
+  launch_cols<true>(f, buf, 1, 0.0, 0, 0.0);
+  launch_cols<true>(f, buf, 0, 0.0, 1, beta);
+  double var = 0.0;
+  rc = field_end(f, buf, r2c, r2c_on_device, &var);
+  if (rc == BEAM_OK && sigma) *sigma = pow(var, 0.5);
+  return rc;
+}
+
+extern "C" int beam_gpu_field_ingest(beam_gpu_ctx *ctx, long NN, double LL, double beta, const double *cube,
+                                     int cube_on_device, double *r2c, int r2c_on_device) {
+  if (!ctx || !cube || !r2c || !std::isfinite(beta)) {
+    set_detail("field ingest: null context or buffer, or non-finite beta");
+    return BEAM_EINVAL;
+  }
+  FieldRun f;
+  int rc = field_begin(ctx, NN, LL, f);
+  if (rc != BEAM_OK) return rc;
+  double *buf = nullptr;
+  if ((rc = field_out(f, r2c, r2c_on_device, &buf)) != BEAM_OK) return rc;
+  const long N = NN;
+  const double *src = cube;
+  long pitch = N;
+  if (!cube_on_device) {  // host rows into the padded buffer
+    cudaError_t e = cudaMemcpy2DAsync(buf, sizeof(double) * (N + 2), cube, sizeof(double) * N, sizeof(double) * N,
+                                      (size_t)N * N, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+      if (!r2c_on_device) cudaFree(buf);
+      set_detail(std::string("field ingest: ") + cudaGetErrorString(e));
+      return BEAM_ECUDA;
+    }
+    src = buf;
+    pitch = N + 2;
+  }
+  // Get_Modes (x LL^3, r2c: rows, axis 1, axis 0) and RSD on the last store
+  launch_rows_r2c(f, buf, src, pitch, false, 0.0, pow(LL, 3.));
+  launch_cols<true>(f, buf, 1, 0.0, 0, 0.0);
+  launch_cols<true>(f, buf, 0, 0.0, 1, beta);
+  return field_end(f, buf, r2c, r2c_on_device, nullptr);
+}

@@ -203,6 +203,11 @@ struct beam_gpu_ctx {
   int num_sms = 0;
   size_t smem_optin = 0;
   beam::Lane lane;
+  // field generator / ingestion workspace (twiddles, row sums, variance), kept
+  // between calls; launches of the last field call
+  void *field_ws = nullptr;
+  size_t field_ws_bytes = 0;
+  int field_launches = 0;
 };
 
 struct beam_gpu_plan {

@@ -283,6 +283,34 @@ BEAM_API int beam_gpu_server_memory(const beam_gpu_server *srv, size_t *now, siz
 BEAM_API int beam_gpu_power_multipoles(beam_gpu_ctx *ctx, long NN, double LL, int Nbin, const double *r2c,
                                        int r2c_on_device, double *out);
 
+/* Field ingestion on the device. Both calls write the r2c buffer
+ * double[NN][NN][NN+2] that beam_gpu_run reads (the reference's on-disk field
+ * format, generate_field.c:100-109), into device memory when r2c_on_device is
+ * set (the buffer can go straight to beam_gpu_run with r2c_on_device) or
+ * host memory otherwise. NN = 2^a 3^b, even, in [4, 1024]. Both run on the
+ * context's stream and return when the buffer is complete. */
+
+/* The reference's field generator `field NN NRi` (generate_field.c:78-88;
+ * replaces Fill_Modes, Make_Image, Non_Gauss, Get_Modes and RSD of
+ * ngrf_2d_funcs.c:341-584,734-765): Gaussian modes of amplitude
+ * sqrt((NN LL)^3/2 k^-2), the real image, x += ff (x^2 - var), x LL^3, the r2c
+ * transform and the (1 + beta mu^2) redshift-space factor. The reference
+ * program uses LL = 0.56, ff = 0.5, beta = 1 and seed = 100020 + 146 NRi
+ * (generate_field.c:45-50). The reference draws its modes from GSL's
+ * MT19937 + ziggurat; here draw n of the fill order is a counter-based normal
+ * deviate (Philox4x32-10 with key = seed, then Box-Muller), so a seed gives
+ * the same field on every device but not the GSL field. sigma (may be NULL)
+ * receives the Gaussian image's rms, which the reference prints. */
+BEAM_API int beam_gpu_field_generate(beam_gpu_ctx *ctx, long NN, unsigned long long seed, double LL, double ff,
+                                     double beta, double *r2c, int r2c_on_device, double *sigma);
+
+/* A real-space density cube double[NN][NN][NN] (host or device memory; it
+ * must not overlap r2c) to the r2c buffer: Get_Modes (x LL^3, the 3D r2c
+ * transform, ngrf_2d_funcs.c:534-550) and RSD with beta (ngrf_2d_funcs.c:734-765;
+ * beta = 0 leaves the modes as transformed). */
+BEAM_API int beam_gpu_field_ingest(beam_gpu_ctx *ctx, long NN, double LL, double beta, const double *cube,
+                                   int cube_on_device, double *r2c, int r2c_on_device);
+
 /* Human-readable text for an error code. */
 BEAM_API const char *beam_gpu_strerror(int code);
 

@@ -111,6 +111,20 @@ double orc_triple_product(long NN, const double *F1, const double *F2, const dou
  * kmode, P0, P2, P4, P6, mode count (the columns of calpow_mom.c:115). */
 int orc_power_multipoles(long NN, double LL, int Nbin, const double *r2c, double *out);
 
+/* Field generator (field_oracle.c). Normal deviates: orc_normal of
+ * philox_normal.h, draw n of the stream with the given seed.
+ *
+ * Fill_Modes (ngrf_2d_funcs.c:341-510): the Gaussian modes of the half-complex
+ * array A[N][N][N/2+1] (interleaved re,im), amplitude sqrt(vol/2 * k^-2). */
+void orc_field_fill_modes(long N, uint64_t seed, double LL, double *A);
+/* generate_field.c:81-86: Fill_Modes, Make_Image, Non_Gauss (x += ff (x^2 - var)),
+ * Get_Modes, RSD(beta), into the r2c buffer double[N][N][N+2]; sigma = sqrt(var)
+ * of the Gaussian image. Returns 0, or -1 on invalid arguments. */
+int orc_field_generate(long N, uint64_t seed, double LL, double ff, double beta, double *r2c, double *sigma);
+/* A real-space cube double[N][N][N] to the r2c buffer: Get_Modes (x LL^3, r2c
+ * transform, ngrf_2d_funcs.c:534-550) and RSD(beta) (ngrf_2d_funcs.c:734-765). */
+int orc_field_ingest(long N, double LL, double beta, const double *cube, double *r2c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -144,3 +144,39 @@ void orc_fft2d_threads(long n0, long n1, int sign, double *data, int nthreads) {
   table_free(&t0);
   table_free(&t1);
 }
+
+void orc_r2c_3d(long n0, long n1, long n2, double *padded) {
+  const long nh = n2 / 2 + 1, pitch = 2 * nh;
+  double *z = (double *)calloc(2 * (size_t)n0 * n1 * n2, sizeof(double));
+  for (long ij = 0; ij < n0 * n1; ++ij)
+    for (long k = 0; k < n2; ++k) z[2 * (ij * n2 + k)] = padded[ij * pitch + k];
+  orc_fft3d(n0, n1, n2, -1, z);
+  for (long ij = 0; ij < n0 * n1; ++ij)
+    for (long k = 0; k < nh; ++k) {
+      padded[ij * pitch + 2 * k] = z[2 * (ij * n2 + k)];
+      padded[ij * pitch + 2 * k + 1] = z[2 * (ij * n2 + k) + 1];
+    }
+  free(z);
+}
+
+void orc_c2r_3d(long n0, long n1, long n2, double *padded) {
+  const long nh = n2 / 2 + 1, pitch = 2 * nh;
+  double *z = (double *)malloc(sizeof(double) * 2 * (size_t)n0 * n1 * n2);
+  for (long i = 0; i < n0; ++i)
+    for (long j = 0; j < n1; ++j)
+      for (long k = 0; k < n2; ++k) {
+        double *dst = z + 2 * ((i * n1 + j) * n2 + k);
+        if (k < nh) {
+          dst[0] = padded[(i * n1 + j) * pitch + 2 * k];
+          dst[1] = padded[(i * n1 + j) * pitch + 2 * k + 1];
+        } else {
+          const long ic = (n0 - i) % n0, jc = (n1 - j) % n1, kc = n2 - k;
+          dst[0] = padded[(ic * n1 + jc) * pitch + 2 * kc];
+          dst[1] = -padded[(ic * n1 + jc) * pitch + 2 * kc + 1];
+        }
+      }
+  orc_fft3d(n0, n1, n2, +1, z);
+  for (long ij = 0; ij < n0 * n1; ++ij)
+    for (long k = 0; k < n2; ++k) padded[ij * pitch + k] = z[2 * (ij * n2 + k)];
+  free(z);
+}

@@ -32,6 +32,20 @@ void orc_fft2d_threads(long n0, long n1, int sign, double *data, int nthreads);
 /* In-place 3D DFT of an n0 x n1 x n2 row-major complex array (interleaved re,im). */
 void orc_fft3d(long n0, long n1, long n2, int sign, double *data);
 
+/* The two real 3D transforms the reference's field generator plans in place on
+ * a double[n0][n1][n2+2] buffer (fftw_plan_dft_r2c_3d / fftw_plan_dft_c2r_3d,
+ * generate_field.c:78-79), by their FFTW definitions:
+ *   r2c: the unnormalised forward DFT (sign -1) of the n0*n1*n2 real values
+ *        x[i][j][k] (k < n2 of each padded row), keeping the n2/2+1 complex
+ *        values k2 <= n2/2 of each row;
+ *   c2r: the unnormalised backward DFT (sign +1) of the Hermitian extension
+ *        X[i][j][n2-k] = conj X[-i][-j][k] of the half spectrum; the real parts
+ *        are written to k < n2 of each row (the imaginary parts of an exactly
+ *        Hermitian input cancel).
+ * Both go through one complex n0*n1*n2 array. */
+void orc_r2c_3d(long n0, long n1, long n2, double *padded);
+void orc_c2r_3d(long n0, long n1, long n2, double *padded);
+
 #ifdef __cplusplus
 }
 #endif

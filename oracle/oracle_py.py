@@ -82,6 +82,8 @@ def lib() -> ctypes.CDLL:
         L.orc_triple_product.argtypes = [ctypes.c_long, dp, dp, dp, ctypes.c_int, ctypes.c_int]
         L.orc_triple_product.restype = ctypes.c_double
         L.orc_fft2d.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_int, dp]
+        L.orc_r2c_3d.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, dp]
+        L.orc_c2r_3d.argtypes = [ctypes.c_long, ctypes.c_long, ctypes.c_long, dp]
         _lib = L
     return _lib
 
@@ -161,6 +163,67 @@ def power_multipoles(r2c: np.ndarray, NN: int, LL: float = 0.56, Nbin: int = 10)
     if L.orc_power_multipoles(NN, LL, Nbin, _dp(np.ascontiguousarray(r2c, dtype=np.float64)), _dp(out)) != 0:
         raise ValueError("orc_power_multipoles: invalid arguments")
     return dict(zip(("k", "P0", "P2", "P4", "P6", "count"), out.reshape(6, Nbin)))
+
+
+def field_seed(NRi: int) -> int:
+    """generate_field.c:49: the generator's seed for realization NRi."""
+    return 100020 + 146 * NRi
+
+
+def field_generate(NN: int, seed: int, LL: float = 0.56, ff: float = 0.5, beta: float = 1.0):
+    """generate_field.c:81-86 (Fill_Modes .. RSD) -> (r2c double[NN][NN][NN+2], sigma).
+    The Gaussian draws are the Philox stream of oracle/philox_normal.h."""
+    L = lib()
+    L.orc_field_generate.argtypes = [ctypes.c_long, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.orc_field_generate.restype = ctypes.c_int
+    out = np.zeros((NN, NN, NN + 2))
+    sigma = ctypes.c_double()
+    if L.orc_field_generate(NN, seed, LL, ff, beta, _dp(out), ctypes.byref(sigma)) != 0:
+        raise ValueError("orc_field_generate: invalid arguments")
+    return out, sigma.value
+
+
+def field_fill_modes(NN: int, seed: int, LL: float = 0.56) -> np.ndarray:
+    """ngrf_2d_funcs.c:341-510 -> the Gaussian half-complex modes, complex [NN][NN][NN/2+1]."""
+    L = lib()
+    L.orc_field_fill_modes.argtypes = [ctypes.c_long, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    out = np.zeros((NN, NN, NN // 2 + 1), dtype=np.complex128)
+    L.orc_field_fill_modes(NN, seed, LL, out.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return out
+
+
+def field_ingest(cube: np.ndarray, LL: float = 0.56, beta: float = 1.0) -> np.ndarray:
+    """Get_Modes + RSD (ngrf_2d_funcs.c:534-550,734-765) of a real cube [NN][NN][NN] -> r2c buffer."""
+    cube = np.ascontiguousarray(cube, dtype=np.float64)
+    NN = cube.shape[0]
+    L = lib()
+    L.orc_field_ingest.argtypes = [ctypes.c_long, ctypes.c_double, ctypes.c_double,
+                                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.orc_field_ingest.restype = ctypes.c_int
+    out = np.zeros((NN, NN, NN + 2))
+    if L.orc_field_ingest(NN, LL, beta, _dp(cube), _dp(out)) != 0:
+        raise ValueError("orc_field_ingest: invalid arguments")
+    return out
+
+
+def r2c_3d(cube: np.ndarray) -> np.ndarray:
+    """The oracle's in-place 3D r2c transform (FFTW's fftw_plan_dft_r2c_3d definition) of a real cube."""
+    cube = np.asarray(cube, dtype=np.float64)
+    NN = cube.shape[0]
+    buf = np.zeros((NN, NN, NN + 2))
+    buf[:, :, :NN] = cube
+    lib().orc_r2c_3d(NN, NN, NN, _dp(buf))
+    return buf.view(np.complex128)
+
+
+def c2r_3d(half: np.ndarray) -> np.ndarray:
+    """The oracle's 3D c2r transform (FFTW's fftw_plan_dft_c2r_3d definition) of a half spectrum."""
+    half = np.ascontiguousarray(half, dtype=np.complex128)
+    NN = half.shape[0]
+    buf = half.view(np.float64).copy()
+    lib().orc_c2r_3d(NN, NN, NN, _dp(buf))
+    return buf[:, :, :NN].copy()
 
 
 def biana(tri: np.ndarray, NN: int, LL: float = 1.0) -> np.ndarray:

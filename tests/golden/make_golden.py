@@ -19,8 +19,14 @@ pk_<case>.npz holds the reference's power-spectrum multipoles of the same field
 (calpow_mom.c with funcs.c:860-1074, built as oracle/_ref/calpow_ref, printing
 %.17e): pk float64[n, 6] = k, P0, P2, P4, P6, mode count of the printed bins.
 
-Usage: python tests/golden/make_golden.py [--pk] [case ...]   (default: all cases;
---pk makes only the pk_<case>.npz files)
+field_<case>.npz holds the r2c buffer written by the reference's field
+generator (generate_field.c + ngrf_2d_funcs.c, built unmodified as
+oracle/_ref/field_ref against the FFTW shim and the GSL stand-in, whose normal
+deviates are the Philox stream of oracle/philox_normal.h): r2c
+float64[NN][NN][NN+2] and the printed sigma.
+
+Usage: python tests/golden/make_golden.py [--pk | --field] [case ...]   (default:
+all cases; --pk makes only the pk_<case>.npz files, --field only the field ones)
 Needs the reference sources (to build oracle/_ref) -- run where they exist.
 """
 from __future__ import annotations
@@ -43,6 +49,10 @@ from barbie_b200.synth import realization_seed, synth_field, write_field  # noqa
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "barbie_ref")
 PK_BIN = os.path.join(ROOT, "oracle", "_ref", "calpow_ref")
+FIELD_BIN = os.path.join(ROOT, "oracle", "_ref", "field_ref")
+
+# name: (NN, realization) of the generator fixtures; 24 = 2^3 * 3 takes a radix-3 stage
+FIELD_CASES = {"n16_r1": (16, 1), "n24_r3": (24, 3)}
 
 # name: (NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, realization)
 CASES = {
@@ -103,15 +113,36 @@ def run_pk_case(name: str, scratch: str) -> str:
     return out
 
 
+def run_field_case(name: str, scratch: str) -> str:
+    NN, r = FIELD_CASES[name]
+    work = os.path.join(scratch, "field_" + name)
+    shutil.rmtree(work, ignore_errors=True)
+    os.makedirs(os.path.join(work, f"ResFiles_N{NN}", "data_files"))
+    res = subprocess.run([FIELD_BIN, str(NN), str(r)], cwd=work, capture_output=True, text=True, check=True)
+    sigma = float(res.stdout.split("sigma =")[1].split()[0])
+    r2c = np.fromfile(os.path.join(work, f"ResFiles_N{NN}", "data_files", f"field_N{NN}_R{r}.txt"))
+    out = os.path.join(HERE, f"field_{name}.npz")
+    np.savez_compressed(out, r2c=r2c.reshape(NN, NN, NN + 2), sigma=sigma, config=np.array([NN, r], dtype=np.int64))
+    shutil.rmtree(work, ignore_errors=True)
+    print(f"field_{name}: sigma {sigma} -> {out}")
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("cases", nargs="*", default=list(CASES))
     ap.add_argument("--pk", action="store_true", help="only the power-spectrum multipole fixtures")
+    ap.add_argument("--field", action="store_true", help="only the field generator fixtures")
     ap.add_argument("--scratch", default=os.path.join(HERE, ".scratch"))
     args = ap.parse_args()
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
     if not os.path.exists(REF_BIN):
         sys.exit("oracle/_ref/barbie_ref is missing: the reference sources are needed to build it")
+    if args.field:
+        for c in (args.cases if args.cases != list(CASES) else list(FIELD_CASES)):
+            run_field_case(c, args.scratch)
+        shutil.rmtree(args.scratch, ignore_errors=True)
+        return
     for c in args.cases:
         if args.pk:
             run_pk_case(c, args.scratch)
