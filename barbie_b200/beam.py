@@ -179,6 +179,12 @@ class Context:
         """cudaStream_t the library launches on (address)."""
         return _lib.beam_gpu_stream(self._h) or 0
 
+    def field_launches(self) -> int:
+        """Kernels the last field generate / ingest call launched."""
+        _lib.beam_gpu_field_launches.argtypes = [ctypes.c_void_p]
+        _lib.beam_gpu_field_launches.restype = ctypes.c_int
+        return int(_lib.beam_gpu_field_launches(self._h))
+
     def close(self) -> None:
         """Destroy the context; plans made on it are destroyed first."""
         if getattr(self, "_h", None):

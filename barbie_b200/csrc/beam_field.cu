@@ -5,13 +5,17 @@
 //
 // 3D transforms. A 3D DFT of the padded r2c layout is three passes of batched
 // 1D transforms, one per axis, each reading and writing the buffer once:
-//   * rows (last axis, contiguous): r2c / c2r of M rows per CTA;
+//   * rows (last axis, contiguous): r2c / c2r of M rows per CTA, each row's N
+//     reals taken as N/2 complex pairs (one half-length complex FFT and a
+//     twist);
 //   * columns (axes 0 and 1, strided): M adjacent k-columns per CTA, so every
 //     global access is M consecutive complex values (128 B at M = 8).
-// A CTA stages its M lines in shared memory and runs a Stockham autosort FFT
-// (radix 4, 2 and 3 stages, N = 2^a 3^b) between two buffers, one butterfly
-// per thread per step, with the twiddle table exp(-2 pi i n / N) in shared
-// memory. The transforms are unnormalised, FFTW's convention.
+// A CTA stages its M lines in shared memory with 16-byte asynchronous copies
+// (the whole tile in flight at once) and runs a Stockham autosort FFT (radix
+// 4, 2 and 3 stages, N = 2^a 3^b) between two buffers, one butterfly per
+// thread per step, with the twiddle table exp(-2 pi i n / N) in shared memory.
+// The transforms are unnormalised, FFTW's convention. HBM-bound: each pass
+// moves 2 x 16 N^2 (N/2+1) bytes.
 //
 // Fused element work (no extra passes):
 //   * Make_Image's division by vol on the load of the first backward pass;
@@ -43,27 +47,40 @@ constexpr long FIELD_MAX_N = 1024;
 constexpr long FFT_TILE = 3072;  // complex values of one staging buffer (lines x length)
 
 struct FftGeom {
-  int N;  // line length
-  int M;  // lines per CTA
-  int nst;
-  int R[FFT_MAX_STAGES];
+  int N;         // line length
+  int M;         // lines per CTA (a power of two)
+  int lgM;       // log2 M
+  int nst;       // stages
+  unsigned rad;  // radix of stage s: 2-bit code (rad >> 2s) & 3, 0 -> 4, 1 -> 2, 2 -> 3
 };
+
+// n / d as a multiply-high: exact for n, d < 2^16 (n d < 2^32), d >= 2
+struct FastDiv {
+  unsigned d, mul;
+};
+static FastDiv fast_div(unsigned d) { return FastDiv{d, (unsigned)(((1ull << 32) + d - 1) / d)}; }
+__device__ __forceinline__ unsigned fdiv(unsigned n, FastDiv f) { return __umulhi(n, f.mul); }
+
+__host__ __device__ __forceinline__ int fft_radix(unsigned rad, int s) {
+  const unsigned c = (rad >> (2 * s)) & 3u;
+  return c == 0 ? 4 : (c == 1 ? 2 : 3);
+}
 
 // N = 2^a 3^b: radix-4 stages, one radix-2 stage for an odd power of two, then radix-3
 static bool fft_geom(long N, FftGeom *g) {
   if (N < 2 || N > FIELD_MAX_N) return false;
   g->N = (int)N;
   g->M = 16;
-  while (g->M > 1 && N * g->M > FFT_TILE) g->M >>= 1;
+  g->lgM = 4;
+  while (g->M > 1 && N * g->M > FFT_TILE) g->M >>= 1, g->lgM--;
   g->nst = 0;
+  g->rad = 0;
   long n = N;
-  while (n % 4 == 0 && g->nst < FFT_MAX_STAGES) g->R[g->nst++] = 4, n /= 4;
-  while (n % 2 == 0 && g->nst < FFT_MAX_STAGES) g->R[g->nst++] = 2, n /= 2;
-  while (n % 3 == 0 && g->nst < FFT_MAX_STAGES) g->R[g->nst++] = 3, n /= 3;
+  while (n % 4 == 0 && g->nst < FFT_MAX_STAGES) g->nst++, n /= 4;
+  while (n % 2 == 0 && g->nst < FFT_MAX_STAGES) g->rad |= 1u << (2 * g->nst++), n /= 2;
+  while (n % 3 == 0 && g->nst < FFT_MAX_STAGES) g->rad |= 2u << (2 * g->nst++), n /= 3;
   return n == 1;
 }
-
-static size_t fft_smem(const FftGeom &g) { return sizeof(double2) * ((size_t)g.N + 2 * (size_t)g.N * g.M); }
 
 // ---------------------------------------------------------------------------
 // Counter-based normal deviates: draw n of the stream with seed s is
@@ -168,69 +185,76 @@ __global__ void k_field_fill(double2 *__restrict__ A, long N, unsigned long long
 }
 
 // ---------------------------------------------------------------------------
-// Stockham FFT of the CTA's M lines, from b0 into the returned buffer.
-// Stage s of radix R (Ns = product of the earlier radices): butterfly j reads
-// positions j + r N/R, applies the twiddles exp(-+2 pi i r (j mod Ns)/(Ns R)),
-// and writes positions (j - j mod Ns) R + j mod Ns + r Ns.
-// ROWS: line m at b[m N + p] (rows of the last axis); else b[p M + m].
+// Staging: 16-byte asynchronous copies global -> shared (cp.async), so a CTA's
+// whole tile is in flight at once.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Stockham FFT of the CTA's M lines of length g.N, from b0 into the returned
+// buffer; element p of line m is at m sm + p sp (columns: sm = 1, sp = M;
+// rows: sm = an odd pitch, sp = 1). Stage s of radix R (Ns = product of the
+// earlier radices): butterfly j reads positions j + r N/R, applies the
+// twiddles exp(-+2 pi i r (j mod Ns)/(Ns R)), and writes positions
+// (j - j mod Ns) R + j mod Ns + r Ns. Consecutive threads take consecutive
+// lines of one butterfly, so a quarter warp touches 8 distinct bank groups.
+// tw holds exp(-2 pi i t/(tws N)).
 template <bool FWD>
 __device__ __forceinline__ double2 twmul(double2 a, double2 w) {
   const double wy = FWD ? w.y : -w.y;
-  return make_double2(a.x * w.x - a.y * wy, a.x * wy + a.y * w.x);
+  return make_double2(__fma_rn(a.x, w.x, -(a.y * wy)), __fma_rn(a.x, wy, a.y * w.x));
 }
 
-template <bool FWD, bool ROWS>
-__device__ double2 *fft_lines(double2 *b0, double2 *b1, const double2 *__restrict__ tw, const FftGeom &g) {
+template <bool FWD>
+__device__ double2 *fft_lines(double2 *b0, double2 *b1, const double2 *__restrict__ tw, int tws, const FftGeom &g,
+                              int sm, int sp) {
   const int N = g.N, M = g.M;
   int Ns = 1;
   for (int s = 0; s < g.nst; ++s) {
-    const int R = g.R[s], NR = N / R, tstr = N / (Ns * R);
+    const int R = fft_radix(g.rad, s), NR = N / R, tstr = tws * (N / (Ns * R));
+    const bool pow2 = (Ns & (Ns - 1)) == 0;
     for (int b = threadIdx.x; b < M * NR; b += blockDim.x) {
-      int m, j;
-      if (ROWS) {
-        m = b / NR;
-        j = b - m * NR;
-      } else {
-        j = b / M;
-        m = b - j * M;
-      }
-      const int js = j % Ns, o = (j - js) * R + js;
-      auto at = [&](int p) { return ROWS ? m * N + p : p * M + m; };
+      const int m = b & (M - 1), j = b >> g.lgM;
+      const int js = pow2 ? (j & (Ns - 1)) : (j % Ns), o = (j - js) * R + js;
+      const double2 *x = b0 + m * sm;
+      double2 *y = b1 + m * sm;
       if (R == 4) {
-        const double2 a0 = b0[at(j)];
-        const double2 a1 = twmul<FWD>(b0[at(j + NR)], tw[js * tstr]);
-        const double2 a2 = twmul<FWD>(b0[at(j + 2 * NR)], tw[2 * js * tstr]);
-        const double2 a3 = twmul<FWD>(b0[at(j + 3 * NR)], tw[3 * js * tstr]);
+        const double2 a0 = x[j * sp];
+        const double2 a1 = twmul<FWD>(x[(j + NR) * sp], tw[js * tstr]);
+        const double2 a2 = twmul<FWD>(x[(j + 2 * NR) * sp], tw[2 * js * tstr]);
+        const double2 a3 = twmul<FWD>(x[(j + 3 * NR) * sp], tw[3 * js * tstr]);
         const double2 y0 = make_double2(a0.x + a2.x, a0.y + a2.y), y1 = make_double2(a0.x - a2.x, a0.y - a2.y);
         const double2 y2 = make_double2(a1.x + a3.x, a1.y + a3.y), y3 = make_double2(a1.x - a3.x, a1.y - a3.y);
-        b1[at(o)] = make_double2(y0.x + y2.x, y0.y + y2.y);
-        b1[at(o + 2 * Ns)] = make_double2(y0.x - y2.x, y0.y - y2.y);
+        y[o * sp] = make_double2(y0.x + y2.x, y0.y + y2.y);
+        y[(o + 2 * Ns) * sp] = make_double2(y0.x - y2.x, y0.y - y2.y);
         if (FWD) {  // y1 -+ i y3
-          b1[at(o + Ns)] = make_double2(y1.x + y3.y, y1.y - y3.x);
-          b1[at(o + 3 * Ns)] = make_double2(y1.x - y3.y, y1.y + y3.x);
+          y[(o + Ns) * sp] = make_double2(y1.x + y3.y, y1.y - y3.x);
+          y[(o + 3 * Ns) * sp] = make_double2(y1.x - y3.y, y1.y + y3.x);
         } else {
-          b1[at(o + Ns)] = make_double2(y1.x - y3.y, y1.y + y3.x);
-          b1[at(o + 3 * Ns)] = make_double2(y1.x + y3.y, y1.y - y3.x);
+          y[(o + Ns) * sp] = make_double2(y1.x - y3.y, y1.y + y3.x);
+          y[(o + 3 * Ns) * sp] = make_double2(y1.x + y3.y, y1.y - y3.x);
         }
       } else if (R == 2) {
-        const double2 a0 = b0[at(j)];
-        const double2 a1 = twmul<FWD>(b0[at(j + NR)], tw[js * tstr]);
-        b1[at(o)] = make_double2(a0.x + a1.x, a0.y + a1.y);
-        b1[at(o + Ns)] = make_double2(a0.x - a1.x, a0.y - a1.y);
+        const double2 a0 = x[j * sp];
+        const double2 a1 = twmul<FWD>(x[(j + NR) * sp], tw[js * tstr]);
+        y[o * sp] = make_double2(a0.x + a1.x, a0.y + a1.y);
+        y[(o + Ns) * sp] = make_double2(a0.x - a1.x, a0.y - a1.y);
       } else {  // R == 3
         const double c = 0.86602540378443864676;  // sqrt(3)/2
-        const double2 a0 = b0[at(j)];
-        const double2 a1 = twmul<FWD>(b0[at(j + NR)], tw[js * tstr]);
-        const double2 a2 = twmul<FWD>(b0[at(j + 2 * NR)], tw[2 * js * tstr]);
+        const double2 a0 = x[j * sp];
+        const double2 a1 = twmul<FWD>(x[(j + NR) * sp], tw[js * tstr]);
+        const double2 a2 = twmul<FWD>(x[(j + 2 * NR) * sp], tw[2 * js * tstr]);
         const double2 t = make_double2(a1.x + a2.x, a1.y + a2.y), d = make_double2(a1.x - a2.x, a1.y - a2.y);
-        const double2 mm = make_double2(a0.x - 0.5 * t.x, a0.y - 0.5 * t.y);
-        b1[at(o)] = make_double2(a0.x + t.x, a0.y + t.y);
+        const double2 mm = make_double2(__fma_rn(-0.5, t.x, a0.x), __fma_rn(-0.5, t.y, a0.y));
+        y[o * sp] = make_double2(a0.x + t.x, a0.y + t.y);
         if (FWD) {  // mm -+ i c d
-          b1[at(o + Ns)] = make_double2(mm.x + c * d.y, mm.y - c * d.x);
-          b1[at(o + 2 * Ns)] = make_double2(mm.x - c * d.y, mm.y + c * d.x);
+          y[(o + Ns) * sp] = make_double2(__fma_rn(c, d.y, mm.x), __fma_rn(-c, d.x, mm.y));
+          y[(o + 2 * Ns) * sp] = make_double2(__fma_rn(-c, d.y, mm.x), __fma_rn(c, d.x, mm.y));
         } else {
-          b1[at(o + Ns)] = make_double2(mm.x - c * d.y, mm.y + c * d.x);
-          b1[at(o + 2 * Ns)] = make_double2(mm.x + c * d.y, mm.y - c * d.x);
+          y[(o + Ns) * sp] = make_double2(__fma_rn(-c, d.y, mm.x), __fma_rn(c, d.x, mm.y));
+          y[(o + 2 * Ns) * sp] = make_double2(__fma_rn(c, d.y, mm.x), __fma_rn(-c, d.x, mm.y));
         }
       }
     }
@@ -262,20 +286,23 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_cols(ColPass a, FftGeom g, 
   const long outer = blockIdx.x / a.ntile;
   const int k0 = (int)(blockIdx.x % a.ntile) * M, mc = min(M, a.NH - k0);
   double2 *base = a.data + outer * a.outer_stride + k0;
-  for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
   for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
-    const int p = e / M, m = e - p * M;
-    double2 v = make_double2(0.0, 0.0);
-    if (m < mc) {
-      v = base[p * a.elem_stride + m];
-      if (a.in_div > 0) v = make_double2(v.x / a.in_div, v.y / a.in_div);
-    }
-    b0[e] = v;
+    const int p = e >> g.lgM, m = e & (M - 1);
+    if (m < mc)
+      cp_async16(b0 + e, base + p * a.elem_stride + m);
+    else
+      b0[e] = make_double2(0.0, 0.0);
   }
+  for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
+  cp_async_wait_all();
   __syncthreads();
-  const double2 *r = fft_lines<FWD, false>(b0, b1, tw, g);
+  if (a.in_div > 0) {
+    for (int e = threadIdx.x; e < N * M; e += blockDim.x) b0[e] = make_double2(b0[e].x / a.in_div, b0[e].y / a.in_div);
+    __syncthreads();
+  }
+  const double2 *r = fft_lines<FWD>(b0, b1, tw, 1, g, 1, M);
   for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
-    const int p = e / M, m = e - p * M;
+    const int p = e >> g.lgM, m = e & (M - 1);
     if (m >= mc) continue;
     double2 v = r[e];
     if (a.rsd) {  // element (i, j, k) = (p, outer, k0 + m)
@@ -292,7 +319,14 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_cols(ColPass a, FftGeom g, 
   }
 }
 
-// Row pass over the last axis of the padded buffer (N+2 doubles per row).
+// Row passes over the last axis of the padded buffer (N+2 doubles per row).
+// A real row of N values is read as its L = N/2 complex pairs
+// z[n] = x[2n] + i x[2n+1] (its memory layout), so one complex FFT of length L
+// per row with a twist on either side does the real transform:
+//   r2c: Z = FFT_L(z); X[k] = E + W^k O for k = 0..L, W = exp(-2 pi i/N),
+//        E = (Z[k] + conj Z[L-k])/2, O = (Z[k] - conj Z[L-k])/(2i);
+//   c2r: Z[k] = E' + i O', E' = X[k] + conj X[L-k], O' = (X[k] - conj X[L-k]) W^-k
+//        (the imaginary parts of X[0] and X[L] dropped); z = IFFT_L(Z).
 struct RowPass {
   double *data;
   const double *src;  // r2c: rows read from here (data, or a dense real cube)
@@ -301,69 +335,97 @@ struct RowPass {
   const double *var;  // r2c: Non_Gauss with this variance first (nullptr: none)
   double ff, lcube;   // r2c: x += ff (x^2 - var); x *= lcube (ngrf_2d_funcs.c:540-546,580-582)
   double *row_sumsq;  // c2r: per-row sum of x^2 of the output
+  FastDiv divL, divNH;  // by L = N/2 and NH = L + 1
 };
 
-// forward r2c of M rows: real row -> its N/2+1 complex values, in place
+// shared pitch of a staged row of L complex values: odd, so the lines of one
+// butterfly fall in distinct bank groups
+__host__ __device__ __forceinline__ int row_pitch(int L) { return L | 1; }
+
+// g: the half-length geometry (g.N = L); tw: the length-N table
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_r2c(RowPass a, FftGeom g, const double2 *__restrict__ twg) {
   extern __shared__ double2 fsm[];
-  const int N = g.N, M = g.M, NH = N / 2 + 1;
-  double2 *tw = fsm, *b0 = fsm + N, *b1 = b0 + (size_t)N * M;
+  const int L = g.N, M = g.M, N = 2 * L, NH = L + 1, S = row_pitch(L);
+  double2 *tw = fsm, *b0 = fsm + N, *b1 = b0 + (size_t)M * NH;
   const long r0 = (long)blockIdx.x * M;
-  for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
-  const double var = a.var ? *a.var : 0.0;
-  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
-    const int m = e / N, p = e - m * N;
-    const long row = r0 + m;
-    double x = 0.0;
-    if (row < a.nrows) {
-      x = a.src[row * a.src_pitch + p];
-      if (a.var) x += a.ff * (x * x - var);
-      x = x * a.lcube;
-    }
-    b0[e] = make_double2(x, 0.0);
+  for (int e = threadIdx.x; e < M * L; e += blockDim.x) {
+    const int m = (int)fdiv(e, a.divL), n = e - m * L;
+    if (r0 + m < a.nrows)
+      cp_async16(b0 + m * S + n, a.src + (r0 + m) * a.src_pitch + 2 * n);
+    else
+      b0[m * S + n] = make_double2(0.0, 0.0);
   }
+  for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
+  cp_async_wait_all();
   __syncthreads();
-  const double2 *r = fft_lines<true, true>(b0, b1, tw, g);
+  if (a.var || a.lcube != 1.0) {
+    const double var = a.var ? *a.var : 0.0;
+    for (int e = threadIdx.x; e < M * L; e += blockDim.x) {
+      const int m = (int)fdiv(e, a.divL), n = e - m * L;
+      double x = b0[m * S + n].x, y = b0[m * S + n].y;
+      if (a.var) {
+        x += a.ff * (x * x - var);
+        y += a.ff * (y * y - var);
+      }
+      b0[m * S + n] = make_double2(x * a.lcube, y * a.lcube);
+    }
+    __syncthreads();
+  }
+  const double2 *Z = fft_lines<true>(b0, b1, tw, 2, g, S, 1);
   double2 *out = (double2 *)a.data;
-  for (int e = threadIdx.x; e < NH * M; e += blockDim.x) {
-    const int m = e / NH, q = e - m * NH;
-    const long row = r0 + m;
-    if (row < a.nrows) out[row * NH + q] = r[m * N + q];
+  for (int e = threadIdx.x; e < M * NH; e += blockDim.x) {
+    const int m = (int)fdiv(e, a.divNH), k = e - m * NH;
+    if (r0 + m >= a.nrows) continue;
+    const double2 zk = Z[m * S + (k == L ? 0 : k)], zc = Z[m * S + (k == 0 ? 0 : L - k)];
+    const double2 E = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
+    const double2 O = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));  // (zk - conj zc) / (2i)
+    const double2 w = tw[k];
+    out[(r0 + m) * NH + k] = make_double2(__fma_rn(w.x, O.x, __fma_rn(-w.y, O.y, E.x)),
+                                          __fma_rn(w.x, O.y, __fma_rn(w.y, O.x, E.y)));
   }
 }
 
-// backward c2r of M rows: N/2+1 complex values (Hermitian extension, the
-// imaginary parts of k = 0 and N/2 dropped) -> N real values, in place
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_rows_c2r(RowPass a, FftGeom g, const double2 *__restrict__ twg) {
   extern __shared__ double2 fsm[];
-  const int N = g.N, M = g.M, NH = N / 2 + 1;
-  double2 *tw = fsm, *b0 = fsm + N, *b1 = b0 + (size_t)N * M;
+  const int L = g.N, M = g.M, N = 2 * L, NH = L + 1, S = row_pitch(L);
+  double2 *tw = fsm, *b0 = fsm + N, *b1 = b0 + (size_t)M * NH;
   const long r0 = (long)blockIdx.x * M;
   const double2 *in = (const double2 *)a.data;
+  for (int e = threadIdx.x; e < M * NH; e += blockDim.x) {  // the rows' spectra into b1 (pitch NH)
+    const int m = (int)fdiv(e, a.divNH);
+    if (r0 + m < a.nrows)
+      cp_async16(b1 + e, in + r0 * NH + e);
+    else
+      b1[e] = make_double2(0.0, 0.0);
+  }
   for (int p = threadIdx.x; p < N; p += blockDim.x) tw[p] = twg[p];
-  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
-    const int m = e / N, p = e - m * N;
-    const long row = r0 + m;
-    double2 v = make_double2(0.0, 0.0);
-    if (row < a.nrows) {
-      v = in[row * NH + (p <= N / 2 ? p : N - p)];
-      if (p > N / 2) v.y = -v.y;
-      if (p == 0 || p == N / 2) v.y = 0.0;
-    }
-    b0[e] = v;
+  cp_async_wait_all();
+  __syncthreads();
+  for (int e = threadIdx.x; e < M * L; e += blockDim.x) {
+    const int m = (int)fdiv(e, a.divL), k = e - m * L;
+    double2 xk = b1[m * NH + k], xc = b1[m * NH + L - k];
+    if (k == 0) xk.y = 0.0, xc.y = 0.0;  // DC and Nyquist are real
+    const double2 Ep = make_double2(xk.x + xc.x, xk.y - xc.y);
+    const double2 d = make_double2(xk.x - xc.x, xk.y + xc.y);  // xk - conj xc
+    const double2 w = tw[k];                                    // O' = d conj(w)
+    const double2 Op = make_double2(__fma_rn(d.x, w.x, d.y * w.y), __fma_rn(d.y, w.x, -(d.x * w.y)));
+    b0[m * S + k] = make_double2(Ep.x - Op.y, Ep.y + Op.x);
   }
   __syncthreads();
-  const double2 *r = fft_lines<false, true>(b0, b1, tw, g);
-  for (int e = threadIdx.x; e < N * M; e += blockDim.x) {
-    const int m = e / N, p = e - m * N;
-    const long row = r0 + m;
-    if (row < a.nrows) a.data[row * (N + 2) + p] = r[e].x;
+  const double2 *z = fft_lines<false>(b0, b1, tw, 2, g, S, 1);
+  for (int e = threadIdx.x; e < M * L; e += blockDim.x) {
+    const int m = (int)fdiv(e, a.divL), n = e - m * L;
+    if (r0 + m < a.nrows) ((double2 *)(a.data + (r0 + m) * (N + 2)))[n] = z[m * S + n];
   }
   if (a.row_sumsq) {  // one warp per row, lanes in a fixed order
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int m = warp; m < M; m += FFT_THREADS / 32) {
       double s = 0.0;
-      for (int p = lane; p < N; p += 32) s += r[m * N + p].x * r[m * N + p].x;
+      for (int n = lane; n < L; n += 32) {
+        const double2 v = z[m * S + n];
+        s += v.x * v.x;
+        s += v.y * v.y;
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
       if (lane == 0 && r0 + m < a.nrows) a.row_sumsq[r0 + m] = s;
@@ -414,12 +476,15 @@ static void twiddles(long N, std::vector<double2> &tw) {
 struct FieldRun {
   beam_gpu_ctx *ctx;
   long N;
-  FftGeom g;
-  double2 *tw = nullptr;        // device twiddle table
+  FftGeom gc, gr;               // column lines (length N), row lines (length N/2)
+  double2 *tw = nullptr;        // device twiddle table, length N
   double *row_sumsq = nullptr;  // [N^2]
   double *var = nullptr;
   int launches = 0;
 };
+
+static size_t cols_smem(const FftGeom &g) { return sizeof(double2) * ((size_t)g.N + 2 * (size_t)g.N * g.M); }
+static size_t rows_smem(const FftGeom &g) { return sizeof(double2) * (2 * (size_t)g.N + 2 * (size_t)(g.N + 1) * g.M); }
 
 static int field_workspace(FieldRun &f) {
   beam_gpu_ctx *c = f.ctx;
@@ -439,13 +504,13 @@ static int field_workspace(FieldRun &f) {
   std::vector<double2> tw;
   twiddles(f.N, tw);
   BEAM_CUDA(cudaMemcpyAsync(f.tw, tw.data(), sizeof(double2) * f.N, cudaMemcpyHostToDevice, c->stream));
-  // a synchronous host array: wait before it goes out of scope
+  // a pageable host array: wait before it goes out of scope
   BEAM_CUDA(cudaStreamSynchronize(c->stream));
-  const int smem = (int)fft_smem(f.g);
-  BEAM_CUDA(cudaFuncSetAttribute(k_fft_cols<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  BEAM_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  BEAM_CUDA(cudaFuncSetAttribute(k_fft_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  BEAM_CUDA(cudaFuncSetAttribute(k_fft_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  const int sc = (int)cols_smem(f.gc), sr = (int)rows_smem(f.gr);
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_cols<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc));
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_cols<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sc));
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_rows_r2c, cudaFuncAttributeMaxDynamicSharedMemorySize, sr));
+  BEAM_CUDA(cudaFuncSetAttribute(k_fft_rows_c2r, cudaFuncAttributeMaxDynamicSharedMemorySize, sr));
   return BEAM_OK;
 }
 
@@ -458,11 +523,11 @@ static void launch_cols(FieldRun &f, double *buf, int axis, double in_div, int r
   a.outer_stride = axis == 0 ? NH : N * NH;
   a.elem_stride = axis == 0 ? N * NH : NH;
   a.NH = (int)NH;
-  a.ntile = (int)((NH + f.g.M - 1) / f.g.M);
+  a.ntile = (int)((NH + f.gc.M - 1) / f.gc.M);
   a.in_div = in_div;
   a.rsd = rsd;
   a.beta = beta;
-  k_fft_cols<FWD><<<(unsigned)(N * a.ntile), FFT_THREADS, fft_smem(f.g), f.ctx->stream>>>(a, f.g, f.tw);
+  k_fft_cols<FWD><<<(unsigned)(N * a.ntile), FFT_THREADS, cols_smem(f.gc), f.ctx->stream>>>(a, f.gc, f.tw);
   ++f.launches;
 }
 
@@ -476,8 +541,10 @@ static void launch_rows_r2c(FieldRun &f, double *buf, const double *src, long sr
   a.var = nongauss ? f.var : nullptr;
   a.ff = ff;
   a.lcube = lcube;
-  k_fft_rows_r2c<<<(unsigned)((a.nrows + f.g.M - 1) / f.g.M), FFT_THREADS, fft_smem(f.g), f.ctx->stream>>>(a, f.g,
-                                                                                                          f.tw);
+  a.divL = fast_div((unsigned)(f.N / 2));
+  a.divNH = fast_div((unsigned)(f.N / 2 + 1));
+  k_fft_rows_r2c<<<(unsigned)((a.nrows + f.gr.M - 1) / f.gr.M), FFT_THREADS, rows_smem(f.gr), f.ctx->stream>>>(
+      a, f.gr, f.tw);
   ++f.launches;
 }
 
@@ -486,8 +553,10 @@ static void launch_rows_c2r(FieldRun &f, double *buf) {
   a.data = buf;
   a.nrows = f.N * f.N;
   a.row_sumsq = f.row_sumsq;
-  k_fft_rows_c2r<<<(unsigned)((a.nrows + f.g.M - 1) / f.g.M), FFT_THREADS, fft_smem(f.g), f.ctx->stream>>>(a, f.g,
-                                                                                                          f.tw);
+  a.divL = fast_div((unsigned)(f.N / 2));
+  a.divNH = fast_div((unsigned)(f.N / 2 + 1));
+  k_fft_rows_c2r<<<(unsigned)((a.nrows + f.gr.M - 1) / f.gr.M), FFT_THREADS, rows_smem(f.gr), f.ctx->stream>>>(
+      a, f.gr, f.tw);
   ++f.launches;
 }
 
@@ -498,7 +567,8 @@ static int field_begin(beam_gpu_ctx *ctx, long NN, double LL, FieldRun &f) {
   }
   f.ctx = ctx;
   f.N = NN;
-  if (!fft_geom(NN, &f.g) || fft_smem(f.g) > ctx->smem_optin) {
+  if (!fft_geom(NN, &f.gc) || !fft_geom(NN / 2, &f.gr) || cols_smem(f.gc) > ctx->smem_optin ||
+      rows_smem(f.gr) > ctx->smem_optin) {
     set_detail("field: no FFT geometry for this NN");
     return BEAM_EINVAL;
   }
@@ -506,9 +576,15 @@ static int field_begin(beam_gpu_ctx *ctx, long NN, double LL, FieldRun &f) {
   return field_workspace(f);
 }
 
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15) == 0; }
+
 // the output buffer: the caller's device buffer, or a temporary one
 static int field_out(const FieldRun &f, double *r2c, int r2c_on_device, double **buf) {
   if (r2c_on_device) {
+    if (!aligned16(r2c)) {
+      set_detail("field: the device r2c buffer must be 16-byte aligned");
+      return BEAM_EINVAL;
+    }
     *buf = r2c;
     return BEAM_OK;
   }
@@ -535,6 +611,8 @@ static int field_end(FieldRun &f, double *buf, double *r2c, int r2c_on_device, d
 }  // namespace beam
 
 using namespace beam;
+
+extern "C" int beam_gpu_field_launches(const beam_gpu_ctx *ctx) { return ctx ? ctx->field_launches : -1; }
 
 extern "C" int beam_gpu_field_generate(beam_gpu_ctx *ctx, long NN, unsigned long long seed, double LL, double ff,
                                        double beta, double *r2c, int r2c_on_device, double *sigma) {
@@ -573,6 +651,10 @@ extern "C" int beam_gpu_field_ingest(beam_gpu_ctx *ctx, long NN, double LL, doub
                                      int cube_on_device, double *r2c, int r2c_on_device) {
   if (!ctx || !cube || !r2c || !std::isfinite(beta)) {
     set_detail("field ingest: null context or buffer, or non-finite beta");
+    return BEAM_EINVAL;
+  }
+  if (cube_on_device && !aligned16(cube)) {
+    set_detail("field ingest: the device cube must be 16-byte aligned");
     return BEAM_EINVAL;
   }
   FieldRun f;

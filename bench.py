@@ -56,6 +56,7 @@ def parse_args():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched form (64 realizations at NN=256)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving form (Poisson job stream)")
+    ap.add_argument("--no-field", action="store_true", help="skip the field generation / ingestion timing")
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs per precision in the serving stream")
     ap.add_argument("--batch-pool", type=int, default=8, help="distinct fields cycled over the batch")
     return ap.parse_args()
@@ -286,6 +287,7 @@ def run_ours(args):
         cpu = cpu_baseline_port(fields[0], info)
     batched = run_batched(ctx, args) if world == 1 and not args.no_batch else None
     serving = run_serving(ctx, args) if world == 1 and not args.no_serve else None
+    field = run_field(ctx, plan, stream, args) if world == 1 and not args.no_field else None
 
     # kernels per bispectrum as the library counted them in the last run: mode
     # build, one triangle-sum launch per tile class, split reduction, epilogue
@@ -304,6 +306,7 @@ def run_ours(args):
                 "ms_per_step": e2e_total / args.steps},
         "latency": lat, "wall_s": wall, "clocks": clk, "roofline": roofline, "mixed": mixed,
         "cpu_baseline": cpu, "gpu_launches": gpu_launches, "batched": batched, "serving": serving,
+        "field": field,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -352,6 +355,68 @@ def run_batched(ctx, args):
         out[prec] = res
         plan.close()
     return out
+
+
+def run_field(ctx, plan, stream, args):
+    """On-device field ingestion at the bench's NN: the reference generator
+    (beam_gpu_field_generate: fill, 3 backward passes, variance, 3 forward
+    passes) and a real-space cube to the r2c buffer (beam_gpu_field_ingest: 3
+    forward passes), both device-resident, timed with CUDA events on the
+    library's stream around each call; and a job from a real-space cube on the
+    device to its bins (ingest + beam_gpu_run). Every buffer (455 MB) exceeds L2.
+    Roofline: each FFT pass reads and writes the half-complex array once,
+    2 x 16 NN^2 (NN/2+1) bytes; achieved = passes x that / call time."""
+    import torch
+    from barbie_b200 import beam
+    NN = WORKLOAD["NN"]
+    dev = torch.device("cuda", ctx.device)
+    out = torch.empty((NN, NN, NN + 2), dtype=torch.float64, device=dev)
+    cube = torch.randn((NN, NN, NN), dtype=torch.float64, device=dev,
+                       generator=torch.Generator(device=dev).manual_seed(11))
+    reps = max(3, min(args.steps, 10))
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    gen_ms = timed(lambda: beam.generate_field(ctx, NN, beam.field_seed(1), out=out))
+    gen_launches = ctx.field_launches()
+    ing_ms = timed(lambda: beam.ingest_field(ctx, cube, out=out))
+    ing_launches = ctx.field_launches()
+    job_ms = timed(lambda: (beam.ingest_field(ctx, cube, out=out), plan.run(out)))
+    pass_bytes = 2 * 16 * NN * NN * (NN // 2 + 1)
+    peak = hbm_peak()
+    ach = 3 * pass_bytes / (ing_ms / 1e3) / 1e9
+    del out, cube
+    torch.cuda.empty_cache()
+    return {"workload": f"NN={NN} r2c buffer double[{NN}][{NN}][{NN + 2}]; generator constants LL=0.56, ff=0.5, "
+                        "beta=1 (generate_field.c:45-50)",
+            "generate_ms": gen_ms, "generate_launches": gen_launches,
+            "ingest_ms": ing_ms, "ingest_launches": ing_launches,
+            "cube_to_bins_ms": job_ms, "cube_to_bins_per_hour": 3600e3 / job_ms,
+            "roofline": {"kernel": "k_fft_rows_r2c + k_fft_cols (3 passes of one ingestion)", "bound": "hbm",
+                         "achieved": ach, "peak": peak[0], "unit": "GB/s", "frac": ach / peak[0],
+                         "bytes_per_pass": pass_bytes, "peak_source": peak[1]},
+            "timing": "median of CUDA-event times around each call on the library stream"}
+
+
+def hbm_peak():
+    """(GB/s, source) of the measured HBM copy bandwidth."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured copy)"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback 6.65 TB/s (no measured figure)"
 
 
 def run_serving(ctx, args):

@@ -311,6 +311,11 @@ BEAM_API int beam_gpu_field_generate(beam_gpu_ctx *ctx, long NN, unsigned long l
 BEAM_API int beam_gpu_field_ingest(beam_gpu_ctx *ctx, long NN, double LL, double beta, const double *cube,
                                    int cube_on_device, double *r2c, int r2c_on_device);
 
+/* Kernels the last successful field call on this context launched (0 before
+ * any): generate 8 (mode fill, 3 backward passes, variance, 3 forward passes),
+ * ingest 3; -1 for a NULL context. */
+BEAM_API int beam_gpu_field_launches(const beam_gpu_ctx *ctx);
+
 /* Human-readable text for an error code. */
 BEAM_API const char *beam_gpu_strerror(int code);
 
