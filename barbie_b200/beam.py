@@ -70,6 +70,21 @@ class PlanInfo(ctypes.Structure):
                 ("run_bytes", ctypes.c_size_t)]
 
 
+TUNE_MAX, FIELD_TUNE_MAX = 16, 4
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("best", ctypes.c_int), ("tau0", ctypes.c_longlong * TUNE_MAX),
+                ("balance", ctypes.c_double * TUNE_MAX), ("ms", ctypes.c_float * TUNE_MAX),
+                ("items", ctypes.c_int * TUNE_MAX)]
+
+
+class FieldTuneReport(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("best_cols", ctypes.c_int), ("best_rows", ctypes.c_int),
+                ("tile", ctypes.c_int * FIELD_TUNE_MAX), ("cols_ms", ctypes.c_float * FIELD_TUNE_MAX),
+                ("rows_ms", ctypes.c_float * FIELD_TUNE_MAX)]
+
+
 _lib = None
 
 
@@ -300,6 +315,19 @@ class Plan:
                                          n, out.ctypes.data, 0), "beam_gpu_plane_rings")
         return out
 
+    def autotune(self, reps: int = 3) -> dict:
+        """Choose the triangle sums' work decomposition by timing (beam_gpu_plan_autotune).
+
+        Returns the candidates (tau0, balance, ms, items) and the kept one."""
+        _lib.beam_gpu_plan_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(TuneReport)]
+        _lib.beam_gpu_plan_autotune.restype = ctypes.c_int
+        rep = TuneReport()
+        _check(_lib.beam_gpu_plan_autotune(self._h, reps, ctypes.byref(rep)), "beam_gpu_plan_autotune")
+        self.refresh_info()
+        cands = [dict(tau0=rep.tau0[k], balance=rep.balance[k], ms=rep.ms[k], items=rep.items[k])
+                 for k in range(rep.n)]
+        return dict(candidates=cands, best=cands[rep.best])
+
     def last_timings(self) -> dict:
         """Device milliseconds of the stages of the last run (CUDA events)."""
         ms = (ctypes.c_float * 4)()
@@ -330,6 +358,17 @@ def power_multipoles(ctx: "Context", r2c, NN: int, LL: float = 0.56, Nbin: int =
                                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
            "beam_gpu_power_multipoles")
     return dict(zip(PK_COLUMNS, out.reshape(6, Nbin)))
+
+
+def field_autotune(ctx: "Context", NN: int) -> dict:
+    """Choose the field FFT staging tiles for NN by timing (beam_gpu_field_autotune)."""
+    L = load()
+    L.beam_gpu_field_autotune.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.POINTER(FieldTuneReport)]
+    L.beam_gpu_field_autotune.restype = ctypes.c_int
+    rep = FieldTuneReport()
+    _check(L.beam_gpu_field_autotune(ctx._h, NN, ctypes.byref(rep)), "beam_gpu_field_autotune")
+    cands = [dict(tile=rep.tile[k], cols_ms=rep.cols_ms[k], rows_ms=rep.rows_ms[k]) for k in range(rep.n)]
+    return dict(candidates=cands, cols_tile=rep.tile[rep.best_cols], rows_tile=rep.tile[rep.best_rows])
 
 
 def field_seed(NRi: int) -> int:

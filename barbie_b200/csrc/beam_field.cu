@@ -33,6 +33,7 @@
 //
 // The file is compiled without FMA contraction, so the amplitude, scaling and
 // RSD factors round as the reference's C expressions do.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -44,7 +45,7 @@ namespace beam {
 constexpr int FFT_THREADS = 256;
 constexpr int FFT_MAX_STAGES = 12;
 constexpr long FIELD_MAX_N = 1024;
-constexpr long FFT_TILE = 3072;  // complex values of one staging buffer (lines x length)
+constexpr long FFT_TILE = 3072;  // complex values of one staging buffer (lines x length), at most
 
 struct FftGeom {
   int N;         // line length
@@ -66,13 +67,15 @@ __host__ __device__ __forceinline__ int fft_radix(unsigned rad, int s) {
   return c == 0 ? 4 : (c == 1 ? 2 : 3);
 }
 
-// N = 2^a 3^b: radix-4 stages, one radix-2 stage for an odd power of two, then radix-3
-static bool fft_geom(long N, FftGeom *g) {
+// N = 2^a 3^b: radix-4 stages, one radix-2 stage for an odd power of two, then
+// radix-3; M lines per CTA, the largest power of two <= 16 with M N <= tile
+static bool fft_geom(long N, FftGeom *g, long tile = FFT_TILE) {
   if (N < 2 || N > FIELD_MAX_N) return false;
+  tile = std::min(std::max(tile, 1L), FFT_TILE);
   g->N = (int)N;
   g->M = 16;
   g->lgM = 4;
-  while (g->M > 1 && N * g->M > FFT_TILE) g->M >>= 1, g->lgM--;
+  while (g->M > 1 && N * g->M > tile) g->M >>= 1, g->lgM--;
   g->nst = 0;
   g->rad = 0;
   long n = N;
@@ -567,7 +570,10 @@ static int field_begin(beam_gpu_ctx *ctx, long NN, double LL, FieldRun &f) {
   }
   f.ctx = ctx;
   f.N = NN;
-  if (!fft_geom(NN, &f.gc) || !fft_geom(NN / 2, &f.gr) || cols_smem(f.gc) > ctx->smem_optin ||
+  long tc = FFT_TILE, tr = FFT_TILE;  // staging tiles: beam_gpu_field_autotune's choice, if any
+  const auto tuned = ctx->field_tiles.find(NN);
+  if (tuned != ctx->field_tiles.end()) tc = tuned->second.first, tr = tuned->second.second;
+  if (!fft_geom(NN, &f.gc, tc) || !fft_geom(NN / 2, &f.gr, tr) || cols_smem(f.gc) > ctx->smem_optin ||
       rows_smem(f.gr) > ctx->smem_optin) {
     set_detail("field: no FFT geometry for this NN");
     return BEAM_EINVAL;
@@ -681,4 +687,78 @@ extern "C" int beam_gpu_field_ingest(beam_gpu_ctx *ctx, long NN, double LL, doub
   launch_cols<true>(f, buf, 1, 0.0, 0, 0.0);
   launch_cols<true>(f, buf, 0, 0.0, 1, beta);
   return field_end(f, buf, r2c, r2c_on_device, nullptr);
+}
+
+// FFT staging tiles per NN: each candidate tile (lines x length per CTA) timed
+// on one column pass and one row pass over a scratch buffer holding a fixed
+// pattern; the fastest of each is kept for the context's later field calls
+// with this NN. The transforms do not depend on the tile (every line is
+// transformed alike), so results are unchanged bit for bit.
+extern "C" int beam_gpu_field_autotune(beam_gpu_ctx *ctx, long NN, beam_field_tune_report *rep) {
+  if (!ctx) return BEAM_EINVAL;
+  FieldRun f;
+  ctx->field_tiles.erase(NN);
+  int rc = field_begin(ctx, NN, 1.0, f);
+  if (rc != BEAM_OK) return rc;
+  const long N = NN;
+  const size_t n = (size_t)N * N * (N + 2);
+  double *buf = nullptr;
+  size_t got = 0;
+  if ((rc = dev_alloc(&got, &buf, n)) != BEAM_OK) return rc;
+  static const long tiles[] = {768, 1536, 3072};
+  constexpr int NT = (int)(sizeof(tiles) / sizeof(tiles[0]));
+  static_assert(NT <= BEAM_FIELD_TUNE_MAX, "report size");
+  float ms_c[NT], ms_r[NT];
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = BEAM_ECUDA;
+  cudaStream_t st = ctx->stream;
+  for (int k = 0; k < NT && rc == BEAM_OK; ++k) {
+    for (int pass = 0; pass < 2 && rc == BEAM_OK; ++pass) {
+      float best = 1e30f;
+      if (pass == 0 ? !fft_geom(N, &f.gc, tiles[k]) : !fft_geom(N / 2, &f.gr, tiles[k])) {
+        rc = BEAM_EINVAL;
+        break;
+      }
+      if ((rc = field_workspace(f)) != BEAM_OK || (rc = fill_pattern(buf, n, st, ctx->num_sms)) != BEAM_OK) break;
+      for (int r = -1; r < 3; ++r) {  // r = -1: warm-up
+        cudaEventRecord(e0, st);
+        if (pass == 0)
+          launch_cols<true>(f, buf, 0, 0.0, 0, 0.0);
+        else
+          launch_rows_r2c(f, buf, buf, N + 2, false, 0.0, 1.0);
+        cudaEventRecord(e1, st);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+          rc = BEAM_ECUDA;
+          break;
+        }
+        if (r >= 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) best = std::min(best, ms);
+      }
+      (pass == 0 ? ms_c : ms_r)[k] = best;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (rc != BEAM_OK) {
+    set_detail("field autotune: a timing launch failed");
+    return rc;
+  }
+  int bc = 0, br = 0;
+  for (int k = 1; k < NT; ++k) {
+    if (ms_c[k] < ms_c[bc]) bc = k;
+    if (ms_r[k] < ms_r[br]) br = k;
+  }
+  ctx->field_tiles[NN] = std::make_pair((int)tiles[bc], (int)tiles[br]);
+  if (rep) {
+    rep->n = NT;
+    rep->best_cols = bc;
+    rep->best_rows = br;
+    for (int k = 0; k < NT; ++k) {
+      rep->tile[k] = (int)tiles[k];
+      rep->cols_ms[k] = ms_c[k];
+      rep->rows_ms[k] = ms_r[k];
+    }
+  }
+  return BEAM_OK;
 }

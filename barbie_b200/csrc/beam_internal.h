@@ -5,6 +5,8 @@
 #include <stdint.h>
 
 #include <string>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include "beam_gpu.h"
@@ -208,6 +210,9 @@ struct beam_gpu_ctx {
   void *field_ws = nullptr;
   size_t field_ws_bytes = 0;
   int field_launches = 0;
+  // FFT staging tiles (complex values) chosen by beam_gpu_field_autotune per
+  // NN: {column passes, row passes}
+  std::map<long, std::pair<int, int>> field_tiles;
 };
 
 struct beam_gpu_plan {
@@ -227,6 +232,12 @@ struct beam_gpu_plan {
   beam::PixelPath *pix = nullptr;        // plane-ring transform tables / pixel method
   beam::RunSlot *main = nullptr;         // slot of beam_gpu_run and friends (ctx->lane)
   beam::RunSlot *batch[2] = {};          // double-buffered slots of beam_gpu_run_batch
+  // triangle-sum work decomposition (build_work): first cap on the in-plane
+  // triangles one CTA walks (split-K over the triangle list), and the number
+  // of items' worth of work per SM the load balance aims at; set by
+  // beam_gpu_plan_autotune
+  long long tau0 = beam::TRI_TAU_MAX;
+  double balance = 8.0;
 };
 
 namespace beam {
@@ -250,6 +261,8 @@ int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n);
 int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n);
 int fetch_results(beam_gpu_plan *p, RunSlot *s, int n);
 int check_status(RunSlot *s);
+// a fixed pseudo-random pattern in [-1, 1) over n doubles (autotuning inputs)
+int fill_pattern(double *v, size_t n, cudaStream_t st, int num_sms);
 int slot_run_graph(beam_gpu_plan *p, RunSlot *s, int n);
 int copy_result(const beam_gpu_plan *p, const RunSlot *s, int r, beam_result *res);
 template <typename T>

@@ -296,11 +296,12 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   double total = 0.0;
   for (int u = 0; u < d.n_used; ++u)
     for (const Group &gr : groups[u]) total += (double)gr.ntiles * 256.0 * (double)(p->tri_first[u + 1] - p->tri_first[u]);
-  const double target = std::max(1.0, total / (std::max(1, p->ctx->num_sms) * 8.0));
-  // Splits per triplet: by work (load balance) and by list length (no CTA
-  // walks more than about tau_max triangles: a CTA's time grows with its
-  // list, not its tiles). Each split keeps a partial sum per combo, so tau_max
-  // starts at TRI_TAU_MAX and doubles while the partial sums would pass
+  const double target = std::max(1.0, total / (std::max(1, p->ctx->num_sms) * p->balance));
+  // Splits per triplet: by work (load balance: about `balance` items' worth of
+  // work per SM) and by list length (no CTA walks more than about tau_max
+  // triangles: a CTA's time grows with its list, not its tiles). Each split
+  // keeps a partial sum per combo, so tau_max starts at the plan's tau0
+  // (TRI_TAU_MAX unless tuned) and doubles while the partial sums would pass
   // max(PART_PER_COMBO x combos, PART_MIN) slots per realization.
   constexpr long long PART_PER_COMBO = 4, PART_MIN = 64LL << 20;
   std::vector<long long> nruns(d.n_used, 0);
@@ -318,7 +319,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     double want = std::max(std::ceil(wmaxu[u] / target), std::ceil((double)nt / (double)tau_max));
     return (int)std::min<double>(std::max(1.0, want), (double)std::max<long long>(1, nruns[u]));
   };
-  long long tau_max = TRI_TAU_MAX;
+  long long tau_max = std::max<long long>(16, p->tau0);
   for (;;) {
     long long slots = 0;
     for (int u = 0; u < d.n_used; ++u) slots += own[u] ? (long long)splits(u, tau_max) * u_ncombo[u] : u_ncombo[u];

@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched form (64 realizations at NN=256)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving form (Poisson job stream)")
     ap.add_argument("--no-field", action="store_true", help="skip the field generation / ingestion timing")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default work decomposition and FFT tiles (no beam_gpu_*_autotune)")
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs per precision in the serving stream")
     ap.add_argument("--batch-pool", type=int, default=8, help="distinct fields cycled over the batch")
     return ap.parse_args()
@@ -192,6 +194,7 @@ def run_ours(args):
     ctx = beam.Context(local)
     plan = beam.Plan(ctx, W["NN"], W["UL_k1"], W["LL_k1"], W["BW_k1"], Nmax=W["Nmax"], Nr=W["Nr"],
                      n_mtbin=W["n_mtbin"])
+    tuning = {"fp64": tune_plan(plan, args)}
     info = plan.info
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
 
@@ -259,6 +262,7 @@ def run_ours(args):
     if not args.no_mixed:
         plan_m = beam.Plan(ctx, W["NN"], W["UL_k1"], W["LL_k1"], W["BW_k1"], Nmax=W["Nmax"], Nr=W["Nr"],
                            n_mtbin=W["n_mtbin"], precision="mixed")
+        tuning["mixed"] = tune_plan(plan_m, args)
         timed_loop(plan_m, dev_fields, args.warmup)
         barrier()
         mt, mtri = timed_loop(plan_m, dev_fields, args.steps)
@@ -306,7 +310,7 @@ def run_ours(args):
                 "ms_per_step": e2e_total / args.steps},
         "latency": lat, "wall_s": wall, "clocks": clk, "roofline": roofline, "mixed": mixed,
         "cpu_baseline": cpu, "gpu_launches": gpu_launches, "batched": batched, "serving": serving,
-        "field": field,
+        "field": field, "autotune": tuning,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -357,6 +361,20 @@ def run_batched(ctx, args):
     return out
 
 
+def tune_plan(plan, args):
+    """beam_gpu_plan_autotune on the plan (work decomposition of the triangle
+    sums chosen by timing on this device), or None with --no-autotune."""
+    if args.no_autotune:
+        return None
+    t0 = time.perf_counter()
+    rep = plan.autotune(reps=3)
+    rep["seconds"] = time.perf_counter() - t0
+    default = [c for c in rep["candidates"] if c["tau0"] == 512 and c["balance"] == 8.0]
+    if default:
+        rep["default_ms"] = default[0]["ms"]
+    return rep
+
+
 def run_field(ctx, plan, stream, args):
     """On-device field ingestion at the bench's NN: the reference generator
     (beam_gpu_field_generate: fill, 3 backward passes, variance, 3 forward
@@ -370,6 +388,7 @@ def run_field(ctx, plan, stream, args):
     from barbie_b200 import beam
     NN = WORKLOAD["NN"]
     dev = torch.device("cuda", ctx.device)
+    tiles = None if args.no_autotune else beam.field_autotune(ctx, NN)
     out = torch.empty((NN, NN, NN + 2), dtype=torch.float64, device=dev)
     cube = torch.randn((NN, NN, NN), dtype=torch.float64, device=dev,
                        generator=torch.Generator(device=dev).manual_seed(11))
@@ -406,7 +425,8 @@ def run_field(ctx, plan, stream, args):
             "roofline": {"kernel": "k_fft_rows_r2c + k_fft_cols (3 passes of one ingestion)", "bound": "hbm",
                          "achieved": ach, "peak": peak[0], "unit": "GB/s", "frac": ach / peak[0],
                          "bytes_per_pass": pass_bytes, "peak_source": peak[1]},
-            "timing": "median of CUDA-event times around each call on the library stream"}
+            "timing": "median of CUDA-event times around each call on the library stream",
+            "autotune": tiles}
 
 
 def hbm_peak():

@@ -311,6 +311,43 @@ BEAM_API int beam_gpu_field_generate(beam_gpu_ctx *ctx, long NN, unsigned long l
 BEAM_API int beam_gpu_field_ingest(beam_gpu_ctx *ctx, long NN, double LL, double beta, const double *cube,
                                    int cube_on_device, double *r2c, int r2c_on_device);
 
+/* Autotuning. No counterpart in the reference (FFTW's planner is the nearest:
+ * FFTW_ESTIMATE, funcs.c:349,546).
+ *
+ * beam_gpu_plan_autotune: the triangle sums' work decomposition -- tau0, the
+ * first cap on the in-plane triangles one CTA walks (the split-K factor of
+ * each ring triplet's triangle list), and balance, the items' worth of work
+ * per SM the load balance aims at -- chosen by timing each candidate's
+ * triangle phase on this device (the plan's tables are rebuilt per candidate,
+ * mode data a fixed pattern, reps timed runs each, best kept). The plan keeps
+ * the fastest; bins agree with the untuned plan to round-off (only the order
+ * of partial sums changes). Takes about (candidates x (rebuild + (reps+1)
+ * runs)); reps <= 0 means 3. Triangle method only. */
+#define BEAM_TUNE_MAX 16
+typedef struct beam_tune_report {
+  int n;                          /* candidates tried */
+  int best;                       /* the one the plan keeps */
+  long long tau0[BEAM_TUNE_MAX];  /* first cap on in-plane triangles per CTA */
+  double balance[BEAM_TUNE_MAX];  /* items of work per SM aimed at */
+  float ms[BEAM_TUNE_MAX];        /* triangle phase (sums + split reduction), best of reps */
+  int items[BEAM_TUNE_MAX];       /* CTA work items of the candidate */
+} beam_tune_report;
+BEAM_API int beam_gpu_plan_autotune(beam_gpu_plan *plan, int reps, beam_tune_report *rep);
+
+/* beam_gpu_field_autotune: the FFT staging tile (lines x length per CTA) of
+ * the field calls' column and row passes for this NN, each candidate timed on
+ * one pass over a scratch buffer (NN^2 (NN+2) doubles, freed on return); the
+ * context's later field calls with this NN use the fastest. Results do not
+ * depend on the tile. */
+#define BEAM_FIELD_TUNE_MAX 4
+typedef struct beam_field_tune_report {
+  int n, best_cols, best_rows;
+  int tile[BEAM_FIELD_TUNE_MAX];       /* complex values staged per CTA */
+  float cols_ms[BEAM_FIELD_TUNE_MAX];  /* one column pass, best of 3 */
+  float rows_ms[BEAM_FIELD_TUNE_MAX];  /* one row pass, best of 3 */
+} beam_field_tune_report;
+BEAM_API int beam_gpu_field_autotune(beam_gpu_ctx *ctx, long NN, beam_field_tune_report *rep);
+
 /* Kernels the last successful field call on this context launched (0 before
  * any): generate 8 (mode fill, 3 backward passes, variance, 3 forward passes),
  * ingest 3; -1 for a NULL context. */

@@ -62,6 +62,11 @@ def test_null_arguments_are_rejected(beamlib):
     assert L.beam_gpu_plan_create(None, None, None) == beamlib.BEAM_EINVAL
     assert L.beam_gpu_run(None, None, 0, None) == beamlib.BEAM_EINVAL
     assert L.beam_gpu_run_batch_ex(None, None, 0, None, 0) == beamlib.BEAM_EINVAL
+    assert L.beam_gpu_plan_autotune(None, 0, None) == beamlib.BEAM_EINVAL
+    assert L.beam_gpu_field_autotune(None, 64, None) == beamlib.BEAM_EINVAL
+    d = ctypes.c_double
+    assert L.beam_gpu_field_generate(None, 64, 1, d(0.56), d(0.5), d(1.0), None, 0, None) == beamlib.BEAM_EINVAL
+    assert L.beam_gpu_field_launches(None) == -1
 
 
 def test_server_host_side_argument_checks(beamlib):
