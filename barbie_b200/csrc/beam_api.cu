@@ -109,6 +109,7 @@ void beam_gpu_destroy(beam_gpu_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->field_ws) cudaFree(ctx->field_ws);
+  if (ctx->scratch) cudaFree(ctx->scratch);
   lane_destroy(&ctx->lane);
   delete ctx;
 }

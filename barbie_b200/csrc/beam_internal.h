@@ -213,6 +213,9 @@ struct beam_gpu_ctx {
   // FFT staging tiles (complex values) chosen by beam_gpu_field_autotune per
   // NN: {column passes, row passes}
   std::map<long, std::pair<int, int>> field_tiles;
+  // small per-context scratch (power-multipole partial sums), kept between calls
+  void *scratch = nullptr;
+  size_t scratch_bytes = 0;
 };
 
 struct beam_gpu_plan {
@@ -261,6 +264,8 @@ int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n);
 int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n);
 int fetch_results(beam_gpu_plan *p, RunSlot *s, int n);
 int check_status(RunSlot *s);
+// the context's scratch buffer, grown to at least bytes (contents undefined)
+int ctx_scratch(beam_gpu_ctx *ctx, size_t bytes, void **out);
 // a fixed pseudo-random pattern in [-1, 1) over n doubles (autotuning inputs)
 int fill_pattern(double *v, size_t n, cudaStream_t st, int num_sms);
 int slot_run_graph(beam_gpu_plan *p, RunSlot *s, int n);

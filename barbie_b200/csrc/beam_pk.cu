@@ -11,11 +11,19 @@
 // the reference's libm powf differs from it by one float ulp on about 0.06% of
 // modes).
 //
-// One CTA per plane i sums its modes into per-bin partials in a fixed order
-// (tiles of PK_THREADS modes; warp w owns bins w, w + warps, ...); a second
-// kernel adds the planes' partials in plane order. HBM-bound: the buffer is
-// read once (NN^2 (NN/2+1) complex128).
+// Rows (fixed i, j) are contiguous and, among the modes a row contributes,
+// |k| -- and so the bin -- never decreases along k. k_pk_rows therefore reads
+// 32 consecutive modes of a row per warp step (coalesced), combines equal
+// bins with a segmented shuffle scan, and the last lane of each bin's segment
+// adds it to the warp's own shared accumulators; each CTA owns a fixed block
+// of rows, so the summation order is fixed and independent of the device.
+// k_pk_total then adds the CTAs' partials in order. For more than
+// PK_FAST_BINS bins the per-plane kernel k_pk_planes (one CTA per plane, a
+// warp per bin over tiles of PK_THREADS modes) is used instead. HBM-bound:
+// the buffer is read once (NN^2 (NN/2+1) complex128).
 #include <cmath>
+#include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "beam_internal.h"
@@ -24,6 +32,9 @@ namespace beam {
 
 constexpr int PK_THREADS = 256;
 constexpr int PK_VALS = 9;  // P0, P2, P4, P6 sums, |k| sum, modes, sum P2^2, P4^2, P6^2
+constexpr int PK_FAST_BINS = 32;
+constexpr int PK_ROWS = 64;       // rows per CTA of k_pk_rows (8 warps x 8)
+constexpr int PK_ROW_LOADS = 4;   // 32-mode steps of a row loaded ahead by k_pk_rows
 
 struct PkMode {
   int d;  // bin, -1 if the mode is not visited or outside the bins
@@ -114,13 +125,213 @@ __global__ void __launch_bounds__(PK_THREADS) k_pk_planes(const double2 *__restr
   for (int q = tid; q < Nbin * PK_VALS; q += PK_THREADS) part[(size_t)i * Nbin * PK_VALS + q] = acc[q];
 }
 
-// Sum of the planes' partials in plane order.
-__global__ void k_pk_total(const double *__restrict__ part, int NN, int Nbin, double *__restrict__ tot) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= Nbin * PK_VALS) return;
+// the include rules of funcs.c:925-1048 for mode (i, j, k): (a, b) of the
+// visited mode, a = -1 if the reference does not visit it
+__device__ __forceinline__ long pk_visit(long i, long j, long k, long N, long *b) {
+  const long half = N / 2;
+  long a = -1;
+  *b = 0;
+  if (k == 0 || k == half) {
+    if (j == 0 || j == half) {
+      if (i >= 1 && i <= half) a = i, *b = j;  // half lines (funcs.c:925-957)
+    } else if (j < half) {
+      a = (i > half) ? N - i : i, *b = j;  // half planes (funcs.c:961-1000)
+    }
+  } else {
+    a = (i > half) ? N - i : i, *b = (j > half) ? N - j : j;  // half cube (funcs.c:1004-1048)
+  }
+  return a;
+}
+
+// Bin edges of the row kernel: t[d] is the smallest float m (|k| in the
+// reference's units) whose bin (int)floorf((float)(log10((double)(m * NN)) /
+// scale)) (funcs.c:941) is at least d, found on the host with the host's
+// log10 by bisection over float bit patterns (the bin is non-decreasing in m).
+// A mode is in bin d iff t[d] <= m < t[d+1], d in [0, Nbin).
+struct PkEdges {
+  float t[PK_FAST_BINS + 1];
+};
+
+__device__ __forceinline__ int pk_bin(float m, const float *t, int Nbin) {
+  if (!(m >= t[0]) || m >= t[Nbin]) return -1;
+  int lo = 0, hi = Nbin;  // t[lo] <= m < t[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (m >= t[mid])
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(PK_THREADS) k_pk_rows(const double2 *__restrict__ r2c, int NN, int Nbin, float fac,
+                                                        PkEdges edges, double *__restrict__ part) {
+  __shared__ double acc[PK_THREADS / 32][PK_FAST_BINS * PK_VALS];
+  __shared__ float te[PK_FAST_BINS + 1];
+  __shared__ double2 zbuf[PK_THREADS / 32][32 * PK_ROW_LOADS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long N = NN, NH = N / 2 + 1, half = N / 2;
+  for (int q = threadIdx.x; q <= Nbin; q += PK_THREADS) te[q] = edges.t[q];
+  for (int q = lane; q < Nbin * PK_VALS; q += 32) acc[warp][q] = 0.0;
+  __syncthreads();
+  // per-lane running sums of the warp's current bin D (warp-uniform), added
+  // to the warp's accumulators by a fixed shuffle tree when the bin changes
+  double r[PK_VALS];
+#pragma unroll
+  for (int t = 0; t < PK_VALS; ++t) r[t] = 0.0;
+  int D = -1;
+  auto flush = [&]() {
+    if (D >= 0) {
+#pragma unroll
+      for (int t = 0; t < PK_VALS; ++t) {
+        double s = r[t];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) acc[warp][D * PK_VALS + t] += s;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < PK_VALS; ++t) r[t] = 0.0;
+  };
+  for (int rr = 0; rr < PK_ROWS / (PK_THREADS / 32); ++rr) {
+    const long row = (long)blockIdx.x * PK_ROWS + warp + (PK_THREADS / 32) * rr;
+    if (row >= N * N) break;
+    const long i = row / N, j = row - i * N;
+    // every mode a row contributes has a = fold(i), b = fold(j) (funcs.c:925-1048)
+    const long a = (i > half) ? N - i : i, b = (j > half) ? N - j : j;
+    const float ab = fac * a * a + fac * b * b;
+    const double2 *rowp = r2c + row * NH;
+    for (long g0 = 0; g0 < NH; g0 += 32 * PK_ROW_LOADS) {
+      // the group's loads first, all in flight at once, into the warp's buffer
+      {
+        double2 zg[PK_ROW_LOADS];
+#pragma unroll
+        for (int q = 0; q < PK_ROW_LOADS; ++q) {
+          const long c = g0 + 32 * q + lane;
+          zg[q] = c < NH ? rowp[c] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int q = 0; q < PK_ROW_LOADS; ++q) zbuf[warp][32 * q + lane] = zg[q];
+        __syncwarp();
+      }
+#pragma unroll 1
+      for (int q = 0; q < PK_ROW_LOADS; ++q) {
+      const long k0 = g0 + 32 * q;
+      if (k0 >= NH) break;
+      const long c = k0 + lane;
+      int d = -1;
+      double v[PK_VALS];
+#pragma unroll
+      for (int t = 0; t < PK_VALS; ++t) v[t] = 0.0;
+      long bb;
+      if (c < NH && pk_visit(i, j, c, N, &bb) >= 0) {
+        const float m = (float)sqrt((double)(ab + fac * c * c));
+        d = pk_bin(m, te, Nbin);
+        if (d >= 0) {
+          const double2 z = zbuf[warp][32 * q + lane];
+          const float mu = (float)((1.0 * c) / (double)(N * m));
+          const float P2 = (float)(0.5 * (3. * mu * mu - 1.));
+          const double m2 = (double)mu * mu;
+          const float mu4 = (float)(m2 * m2), mu6 = (float)(m2 * m2 * m2);
+          const float P4 = (float)(0.125 * (35.0 * mu4 - 30.0 * mu * mu + 3));
+          const float P6 = (float)(0.0625 * (231.0 * mu6 - 315.0 * mu4 + 105.0 * mu * mu - 5));
+          const double pw = (z.x * z.x) + (z.y * z.y);
+          v[0] = pw, v[1] = pw * P2, v[2] = pw * P4, v[3] = pw * P6, v[4] = (double)m, v[5] = 1.0;
+          v[6] = (double)(P2 * P2), v[7] = (double)(P4 * P4), v[8] = (double)(P6 * P6);
+        }
+      }
+      const int dmax = __reduce_max_sync(0xffffffffu, d);
+      if (dmax < 0) continue;  // nothing counted in these 32 modes
+      const int dmin = (int)__reduce_min_sync(0xffffffffu, d >= 0 ? (unsigned)d : 0xffffffffu);
+      if (dmin == dmax && dmax == D) {
+#pragma unroll
+        for (int t = 0; t < PK_VALS; ++t) r[t] += v[t];
+        continue;
+      }
+      flush();
+      if (dmin < dmax) {
+        // the bins below dmax: segmented scan over runs of equal bins (the
+        // counted bins of a row are non-decreasing in k), run tails add
+        const int ds = d < dmax ? d : -1;
+#pragma unroll
+        for (int t = 0; t < PK_VALS; ++t) r[t] = ds >= 0 ? v[t] : 0.0;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const int db = __shfl_up_sync(0xffffffffu, ds, off);
+          const bool same = lane >= off && db == ds;
+#pragma unroll
+          for (int t = 0; t < PK_VALS; ++t) {
+            const double y = __shfl_up_sync(0xffffffffu, r[t], off);
+            if (same) r[t] += y;
+          }
+        }
+        const int dn = __shfl_down_sync(0xffffffffu, ds, 1);
+        if (ds >= 0 && (lane == 31 || dn != ds))
+#pragma unroll
+          for (int t = 0; t < PK_VALS; ++t) acc[warp][ds * PK_VALS + t] += r[t];
+        __syncwarp();
+      }
+      D = dmax;
+#pragma unroll
+      for (int t = 0; t < PK_VALS; ++t) r[t] = d == dmax ? v[t] : 0.0;
+      }
+      __syncwarp();
+    }
+  }
+  flush();
+  __syncthreads();
+  for (int q = threadIdx.x; q < Nbin * PK_VALS; q += PK_THREADS) {
+    double s = 0.0;
+    for (int w = 0; w < PK_THREADS / 32; ++w) s += acc[w][q];
+    part[(size_t)blockIdx.x * Nbin * PK_VALS + q] = s;
+  }
+}
+
+// Sum of nblk partials in a fixed order: one CTA per value, strided thread
+// sums, then a fixed shuffle / shared-memory tree.
+__global__ void __launch_bounds__(256) k_pk_total(const double *__restrict__ part, int nblk, int Nbin,
+                                                  double *__restrict__ tot) {
+  __shared__ double w8[8];
+  const int q = blockIdx.x;
   double s = 0.0;
-  for (int i = 0; i < NN; ++i) s += part[(size_t)i * Nbin * PK_VALS + q];
-  tot[q] = s;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[(size_t)b * Nbin * PK_VALS + q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) w8[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += w8[w];
+    tot[q] = t;
+  }
+}
+
+// the bin the reference gives m (funcs.c:941), as a float so that no value is
+// out of int range
+static float pk_floor_bin(float m, long NN, float scale) { return floorf((float)(log10((double)(m * NN)) / scale)); }
+
+static void pk_edges(long NN, int Nbin, float scale, PkEdges *e) {
+  const float top = 2.0f;  // |k| in these units is at most sqrt(3)/2
+  uint32_t top_bits;
+  memcpy(&top_bits, &top, 4);
+  for (int d = 0; d <= Nbin; ++d) {
+    if (!(pk_floor_bin(top, NN, scale) >= (float)d)) {
+      e->t[d] = INFINITY;
+      continue;
+    }
+    uint32_t lo = 0, hi = top_bits;  // bin(lo) < d <= bin(hi), over non-negative float bit patterns
+    while (hi - lo > 1) {
+      const uint32_t mid = lo + (hi - lo) / 2;
+      float x;
+      memcpy(&x, &mid, 4);
+      if (pk_floor_bin(x, NN, scale) >= (float)d)
+        hi = mid;
+      else
+        lo = mid;
+    }
+    memcpy(&e->t[d], &hi, 4);
+  }
 }
 
 }  // namespace beam
@@ -140,8 +351,6 @@ extern "C" int beam_gpu_power_multipoles(beam_gpu_ctx *ctx, long NN, double LL, 
   double *d_r2c = nullptr, *part = nullptr, *tot = nullptr;
   auto release = [&]() {
     if (!r2c_on_device && d_r2c) cudaFree(d_r2c);
-    if (part) cudaFree(part);
-    if (tot) cudaFree(tot);
   };
   int rc = BEAM_OK;
   const double *src = r2c;
@@ -151,8 +360,15 @@ extern "C" int beam_gpu_power_multipoles(beam_gpu_ctx *ctx, long NN, double LL, 
       rc = BEAM_ECUDA;
     src = d_r2c;
   }
-  if (rc == BEAM_OK) rc = dev_alloc(&bytes, &part, (size_t)NN * Nbin * PK_VALS);
-  if (rc == BEAM_OK) rc = dev_alloc(&bytes, &tot, (size_t)Nbin * PK_VALS);
+  const bool fast = Nbin <= PK_FAST_BINS;
+  const long nblk = fast ? (NN * NN + PK_ROWS - 1) / PK_ROWS : NN;  // partial sums: per CTA or per plane
+  // partial sums and totals in the context's scratch (no allocation per call)
+  void *ws = nullptr;
+  if (rc == BEAM_OK) rc = ctx_scratch(ctx, sizeof(double) * ((size_t)nblk + 1) * Nbin * PK_VALS, &ws);
+  if (rc == BEAM_OK) {
+    part = (double *)ws;
+    tot = part + (size_t)nblk * Nbin * PK_VALS;
+  }
   if (rc != BEAM_OK) {
     release();
     return rc;
@@ -160,10 +376,16 @@ extern "C" int beam_gpu_power_multipoles(beam_gpu_ctx *ctx, long NN, double LL, 
   // the reference's float constants (funcs.c:898-900,922)
   const float fac = 1. / (1. * NN * NN);
   const float scale = log10(0.5 * NN) / Nbin;
-  const size_t smem = sizeof(double) * (size_t)Nbin * PK_VALS;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_pk_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_pk_planes<<<(unsigned)NN, PK_THREADS, smem, st>>>((const double2 *)src, (int)NN, Nbin, fac, scale, part);
-  k_pk_total<<<(unsigned)((Nbin * PK_VALS + 255) / 256), 256, 0, st>>>(part, (int)NN, Nbin, tot);
+  if (fast) {
+    PkEdges edges;
+    pk_edges(NN, Nbin, scale, &edges);
+    k_pk_rows<<<(unsigned)nblk, PK_THREADS, 0, st>>>((const double2 *)src, (int)NN, Nbin, fac, edges, part);
+  } else {
+    const size_t smem = sizeof(double) * (size_t)Nbin * PK_VALS;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_pk_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_pk_planes<<<(unsigned)NN, PK_THREADS, smem, st>>>((const double2 *)src, (int)NN, Nbin, fac, scale, part);
+  }
+  k_pk_total<<<(unsigned)(Nbin * PK_VALS), 256, 0, st>>>(part, (int)nblk, Nbin, tot);
   std::vector<double> q((size_t)Nbin * PK_VALS);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(q.data(), tot, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, st);

@@ -40,6 +40,22 @@ __global__ void k_fill_pattern_f(float *__restrict__ v, size_t n) {
   }
 }
 
+int ctx_scratch(beam_gpu_ctx *ctx, size_t bytes, void **out) {
+  if (ctx->scratch_bytes < bytes) {
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    size_t got = 0;
+    char *p = nullptr;
+    int rc = dev_alloc(&got, &p, bytes);
+    if (rc != BEAM_OK) return rc;
+    ctx->scratch = p;
+    ctx->scratch_bytes = bytes;
+  }
+  *out = ctx->scratch;
+  return BEAM_OK;
+}
+
 int fill_pattern(double *v, size_t n, cudaStream_t st, int num_sms) {
   k_fill_pattern<<<4 * std::max(1, num_sms), 256, 0, st>>>(v, n);
   BEAM_CUDA(cudaGetLastError());

@@ -412,6 +412,9 @@ def run_field(ctx, plan, stream, args):
     ing_ms = timed(lambda: beam.ingest_field(ctx, cube, out=out))
     ing_launches = ctx.field_launches()
     job_ms = timed(lambda: (beam.ingest_field(ctx, cube, out=out), plan.run(out)))
+    # power spectrum multipoles of the device buffer (calpow_mom): one read of the buffer
+    pk_ms = timed(lambda: beam.power_multipoles(ctx, out, NN, LL=0.56, Nbin=10))
+    pk_bytes = 16 * NN * NN * (NN // 2 + 1)
     pass_bytes = 2 * 16 * NN * NN * (NN // 2 + 1)
     peak = hbm_peak()
     ach = 3 * pass_bytes / (ing_ms / 1e3) / 1e9
@@ -426,7 +429,11 @@ def run_field(ctx, plan, stream, args):
                          "achieved": ach, "peak": peak[0], "unit": "GB/s", "frac": ach / peak[0],
                          "bytes_per_pass": pass_bytes, "peak_source": peak[1]},
             "timing": "median of CUDA-event times around each call on the library stream",
-            "autotune": tiles}
+            "autotune": tiles,
+            "power_multipoles": {"ms": pk_ms, "bins": 10, "roofline": {
+                "kernel": "k_pk_planes + k_pk_total", "bound": "hbm", "achieved": pk_bytes / (pk_ms / 1e3) / 1e9,
+                "peak": peak[0], "unit": "GB/s", "frac": pk_bytes / (pk_ms / 1e3) / 1e9 / peak[0],
+                "bytes": pk_bytes}}}
 
 
 def hbm_peak():

@@ -31,10 +31,10 @@ def ctx(beamlib):
     c.close()
 
 
-def check(got, want):
+def check(got, want, p46_atol=1e-8):
     for col in COLS:
         a, b = np.asarray(got[col]), np.asarray(want[col])
-        atol = 1e-8 * np.abs(np.asarray(want["P0"])) if col in ("P4", "P6") else 0.0
+        atol = p46_atol * np.abs(np.asarray(want["P0"])) if col in ("P4", "P6") else 0.0
         assert np.all(np.abs(a - b) <= RTOL[col] * np.abs(b) + atol), (col, a, b)
 
 
@@ -50,15 +50,18 @@ def test_power_multipoles_match_reference(beamlib, ctx, name):
     check({c: got[c][keep] for c in COLS}, {c: ref[:, k] for k, c in enumerate(COLS)})
 
 
-@pytest.mark.parametrize("Nbin", [7, 24])
+@pytest.mark.parametrize("Nbin", [7, 24, 100])  # 100: the per-plane kernel (more than 32 bins)
 def test_power_multipoles_match_oracle_other_bins(beamlib, ctx, oracle, Nbin):
     torch = pytest.importorskip("torch")
     name = "nn96_r20"
     NN = GOLDEN_CASES[name][0]
     f = golden_field(name)
     want = oracle.power_multipoles(f, NN, LL=1.0, Nbin=Nbin)
-    check(beamlib.power_multipoles(ctx, f, NN, LL=1.0, Nbin=Nbin), want)
-    check(beamlib.power_multipoles(ctx, torch.from_numpy(f).cuda(), NN, LL=1.0, Nbin=Nbin), want)
+    # with many narrow bins a bin holds few modes, so one float ulp of mu^4 or
+    # mu^6 on one of them is no longer small beside the bin's P0
+    p46 = 1e-8 if Nbin <= 24 else 1e-6
+    check(beamlib.power_multipoles(ctx, f, NN, LL=1.0, Nbin=Nbin), want, p46)
+    check(beamlib.power_multipoles(ctx, torch.from_numpy(f).cuda(), NN, LL=1.0, Nbin=Nbin), want, p46)
 
 
 def test_calpow_mom_drop_in(tmp_path):
