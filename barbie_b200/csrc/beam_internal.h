@@ -85,6 +85,12 @@ struct TriDesc {
 static_assert(sizeof(TriDesc) % 16 == 0 && TRI_CHUNK <= 31 && TRI_PIECES <= 4, "TriDesc layout");
 constexpr int TRI_TAU_MAX = 512;  // most in-plane triangles walked by one CTA
 
+// The mixed path's mode rows are blocked by 4 columns: block b of a row holds
+// the real parts of columns 4b..4b+3, then their imaginary parts (8 floats).
+// Float offset of the real part of column col within its row; the imaginary
+// part is 4 floats further.
+__host__ __device__ inline int mixed_re(int col) { return ((col >> 2) << 3) | (col & 3); }
+
 // Shared-memory pitch (complex values) of a staged x or z row of L values.
 // The FP64 consumer reads a quarter-warp's 8 lanes as 2 planes x 4 rows with
 // 16-byte loads; rows 2 (mod 8) 16-byte units apart put those 8 lanes on

@@ -449,7 +449,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   });
   std::vector<TriItem> sorted(items.size());
   for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
-  size_t elem = (A == 2) ? 8 : 16;
+  size_t elem = (A == 1) ? 16 : 8;
   size_t budget = p->ctx->smem_optin > 4096 ? p->ctx->smem_optin - 4096 : 48 * 1024;
   for (int n = 0; n <= TRI_WARPS + 1; ++n) d.class_first[n] = 0;
   for (int n = 0; n <= TRI_WARPS; ++n) d.class_stage[n] = 0;
@@ -510,13 +510,17 @@ int build_plan_tables(beam_gpu_plan *p) {
     Q = std::max(Q, 1 + std::max(p1, std::max(std::abs(p2), std::abs(p3))));
   }
   // bulk copies move whole 16-byte units: rows, their starts and lengths are
-  // kept in multiples of A complex values (1 for complex128, 2 for complex64)
-  const int A = (p->cfg.precision == BEAM_PREC_MIXED) ? 2 : 1;
+  // kept in multiples of A complex values (1 for complex128; 4 for the mixed
+  // path's planar rows, whose real and imaginary parts are copied separately
+  // as floats)
+  const int A = (p->cfg.precision == BEAM_PREC_MIXED) ? 4 : 1;
   auto floorA = [A](int v) { return v - (((v % A) + A) % A); };
   auto ceilA = [A, &floorA](int v) { return floorA(v + A - 1); };
   d.Q = Q;
-  d.colbase = Q - 1 + TRI_PAD;
-  d.W = ceilA(2 * Q - 1 + 2 * TRI_PAD);
+  // plane 0 at a column that is a multiple of A (the mixed consumer reads a
+  // tile's 8 planes p1, which start at multiples of 8, as aligned float4s)
+  d.colbase = ceilA(Q - 1 + TRI_PAD);
+  d.W = ceilA(d.colbase + Q + TRI_PAD);
 
   std::vector<int16_t> pixlocal;
   build_modes(g, ring_on, p->ring_first, p->mode_ij, pixlocal);

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstring>
 #include <new>
+#include <type_traits>
 
 #include "beam_device.cuh"
 #include "beam_internal.h"
@@ -32,7 +33,10 @@ struct CplxOf<float2> {
 // sign_2/sign_3 = -1 (barbie.c:332); other columns are zero.
 // srcs[r] for realization r = blockIdx.y: its staged rows [n_modes][Q]
 // (staged = 1) or its full r2c buffer; S rows of realization r start at
-// r * n_modes * W.
+// r * n_modes * W. FP64 rows are complex128[W]; the mixed path's rows are
+// blocked by 4 columns (mixed_re: 4 real parts, then their 4 imaginary
+// parts), so its consumer loads 4 planes' real or imaginary parts at once
+// and multiplies pairs of planes with packed FP32 FMAs.
 template <typename C>
 __global__ void k_build_modes(const double *const *__restrict__ srcs, int staged, const int16_t *__restrict__ mode_ij,
                               const int32_t *__restrict__ mode_neg, int n_modes, int Q, int W, int colbase, int NN,
@@ -54,7 +58,13 @@ __global__ void k_build_modes(const double *const *__restrict__ srcs, int staged
     if (q == 0 && origin) a = make_double2(0.0, 0.0);
     v = CplxOf<C>::make(a.x, q >= 0 ? a.y : -a.y);
   }
-  S[idx] = v;
+  if constexpr (std::is_same<C, float2>::value) {
+    float *row = reinterpret_cast<float *>(S) + (size_t)m * 2 * W;
+    row[mixed_re(w)] = v.x;
+    row[mixed_re(w) + 4] = v.y;
+  } else {
+    S[idx] = v;
+  }
 }
 
 // ----------------------------------------------------------------- epilogue

@@ -84,6 +84,8 @@ __device__ __forceinline__ void tri_issue(const TriArgs &a, const TriItem &it, c
   C *xs = st, *zs = st + TRI_CHUNK * px, *ys = zs + TRI_CHUNK * pz;
   if (lane == 0) mbar_expect_tx(full, (uint32_t)((nt * (it.Lx + it.Lz) + npc * it.Ly) * sizeof(C)));
   __syncwarp();
+  // one copy per row; a mixed row segment starts at a multiple of 4 columns,
+  // i.e. on a whole block of its 4-column real/imaginary layout
   if (lane < nt) {
     const int mx = it.m1 + (int)(m.xz & 0xffffu), mz = it.m3 + (int)(m.xz >> 16);
     bulk_g2s(smem_addr(xs + lane * px), S + (size_t)mx * a.W + it.colx, (uint32_t)(it.Lx * sizeof(C)), full);
@@ -117,11 +119,34 @@ __device__ __forceinline__ double *tri_out(const TriArgs &a, const TriItem &it) 
 // p3_0 + lane), q < TRI_P1, of its tile. Over a piece it accumulates
 // w[q] += x_k1(p1_0+q) * z_k3(p3) (4 FMA; x read warp-wide from one address)
 // and at the end of the piece adds Re(y_k2(-p1_0-q-p3) * w[q]) to its sums.
+// Packed FP32 pairs (fma.rn.f32x2: two independent FP32 FMAs in one
+// instruction, sm_100).
+__device__ __forceinline__ unsigned long long f2pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2unpack(unsigned long long v, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ void fma2(unsigned long long &d, unsigned long long a, unsigned long long b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+}
+
+// Mixed-precision consumer: FP32 FMA with x broadcast. Lane l works on block
+// l / TRI_BW of the tile: plane p3 = p3_0[l / TRI_BW] + l % TRI_BW and the
+// block's 8 planes p1. Staged rows keep the 4-column blocks of the mode rows
+// (4 real parts, then their 4 imaginary parts; mixed_re), so the 8 x values
+// of a triangle are two float4 loads per part and the accumulators of planes
+// (q, q+1) are packed pairs:
+//   Wr(q,q+1) = fma2(Xr(q,q+1), zr, fma2(Xi(q,q+1), -zi, Wr))
+//   Wi(q,q+1) = fma2(Xr(q,q+1), zi, fma2(Xi(q,q+1),  zr, Wi))
+// the same FP32 operations, in the same order, as one FMA pair per plane.
 template <typename C>
 __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem &it, const C *stages, uint64_t *full,
                                                 uint64_t *empty, volatile int *s_fail, int warp, int lane,
                                                 int nch) {
-  typedef typename TriAcc<C>::t acc_t;
+  static_assert(std::is_same<C, float2>::value && TRI_P1 == 8, "the packed consumer is the FP32 path, 8 planes p1");
   const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + lane;
   bool any = false;
 #pragma unroll
@@ -129,7 +154,7 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
   // the lane's block nb: planes p1_0[nb] + q and p3 = p3_0[nb] + lane % TRI_BW
   const int nb = lane / TRI_BW;
   const int p1b = a.tiles[it.tile0 + warp].p1_0[nb], p3 = a.tiles[it.tile0 + warp].p3_0[nb] + lane % TRI_BW;
-  const int ox0 = p1b + a.colbase - it.colx;                          // x reads ox0 + q
+  const int ox0 = p1b + a.colbase - it.colx;                          // x reads ox0 + q (a multiple of 4)
   const int oz = any ? p3 + a.colbase - it.colz : 0;                  // z read
   const int oy0 = any ? -p1b - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
   double sum[TRI_P1];
@@ -141,37 +166,46 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
     const int packed = packed_next;  // piece layout of this chunk, loaded one chunk ahead
     if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
     if (!tri_wait_chunk(a, full, s_fail, c, lane)) return;
-    const C *xs = stages + s * a.stage;
-    const C *zs = xs + TRI_CHUNK * it.Lx;
-    const C *ys = zs + TRI_CHUNK * it.Lz;
+    const float *xs = reinterpret_cast<const float *>(stages + s * a.stage);
+    const float *zs = xs + 2 * TRI_CHUNK * it.Lx;
+    const float *ys = zs + 2 * TRI_CHUNK * it.Lz;
     const int npc = chunk_npc(packed);
     int tt = 0;
     for (int pc = 0; pc < npc; ++pc) {
       const int len = chunk_len(packed, pc);
-      acc_t wr[TRI_P1], wi[TRI_P1];
+      unsigned long long wr[TRI_P1 / 2], wi[TRI_P1 / 2];  // planes (2h, 2h+1)
 #pragma unroll
-      for (int q = 0; q < TRI_P1; ++q) wr[q] = wi[q] = (acc_t)0;
+      for (int h = 0; h < TRI_P1 / 2; ++h) wr[h] = wi[h] = 0ull;
       for (int j = 0; j < len; ++j, ++tt) {
-        const C z = zs[tt * it.Lz + oz];
-        const C *xr = xs + tt * it.Lx + ox0;
-        // x in two halves: the empty asm keeps the compiler from holding all
-        // TRI_P1 values at once, which leaves the sums room in registers
+        const float *zr = zs + 2 * tt * it.Lz + mixed_re(oz);
+        const float z_re = zr[0], z_im = zr[4];
+        const unsigned long long ZR = f2pack(z_re, z_re), ZI = f2pack(z_im, z_im), NZI = f2pack(-z_im, -z_im);
+        const float *xr = xs + 2 * tt * it.Lx + 2 * ox0;  // ox0 is a multiple of 4: block ox0 / 4
 #pragma unroll
-        for (int h = 0; h < TRI_P1; h += TRI_P1 / 2) {
-#pragma unroll
-          for (int q = h; q < h + TRI_P1 / 2; ++q) {
-            const C x = xr[q];
-            wr[q] = fma(x.x, z.x, fma(-x.y, z.y, wr[q]));
-            wi[q] = fma(x.x, z.y, fma(x.y, z.x, wi[q]));
-          }
-          asm volatile("" ::: "memory");
+        for (int g = 0; g < TRI_P1; g += 4) {
+          const float4 re = *reinterpret_cast<const float4 *>(xr + 2 * g);
+          const float4 im = *reinterpret_cast<const float4 *>(xr + 2 * g + 4);
+          const unsigned long long r0 = f2pack(re.x, re.y), r1 = f2pack(re.z, re.w);
+          const unsigned long long i0 = f2pack(im.x, im.y), i1 = f2pack(im.z, im.w);
+          fma2(wr[g / 2], i0, NZI);
+          fma2(wr[g / 2], r0, ZR);
+          fma2(wi[g / 2], i0, ZR);
+          fma2(wi[g / 2], r0, ZI);
+          fma2(wr[g / 2 + 1], i1, NZI);
+          fma2(wr[g / 2 + 1], r1, ZR);
+          fma2(wi[g / 2 + 1], i1, ZR);
+          fma2(wi[g / 2 + 1], r1, ZI);
         }
       }
-      const C *yr = ys + pc * it.Ly + oy0;
+      const float *yr = ys + 2 * pc * it.Ly;
 #pragma unroll
-      for (int q = 0; q < TRI_P1; ++q) {
-        const C y = yr[-q];
-        sum[q] += (double)fma(y.x, wr[q], -y.y * wi[q]);
+      for (int h = 0; h < TRI_P1 / 2; ++h) {
+        float r0, r1, i0, i1;
+        f2unpack(wr[h], r0, r1);
+        f2unpack(wi[h], i0, i1);
+        const float *y0 = yr + mixed_re(oy0 - 2 * h), *y1 = yr + mixed_re(oy0 - 2 * h - 1);
+        sum[2 * h] += (double)fma(y0[0], r0, -y0[4] * i0);
+        sum[2 * h + 1] += (double)fma(y1[0], r1, -y1[4] * i1);
       }
     }
     __syncwarp();
