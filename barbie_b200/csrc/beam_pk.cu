@@ -44,8 +44,12 @@ struct PkMode {
 // funcs.c:932-954 for one mode (a, b, c) of the r2c buffer.
 __device__ __forceinline__ PkMode pk_mode(double2 z, long a, long b, long c, long NN, int Nbin, float fac, float scale) {
   PkMode r;
-  float m = (float)sqrt((double)(fac * a * a + fac * b * b + fac * c * c));
-  float mu = (float)((1.0 * c) / (double)(NN * m));
+  // sqrt and the division are taken in float: the reference rounds their
+  // double results to float, which gives the correctly rounded float result
+  // (double rounding is innocuous for sqrt and division when the wider format
+  // has at least 2p + 2 bits, 53 >= 2 * 24 + 2), i.e. exactly these
+  float m = __fsqrt_rn(fac * a * a + fac * b * b + fac * c * c);
+  float mu = __fdiv_rn((float)c, NN * m);
   float P2 = (float)(0.5 * (3. * mu * mu - 1.));
   const double m2 = (double)mu * mu;
   const float mu4 = (float)(m2 * m2), mu6 = (float)(m2 * m2 * m2);
@@ -226,11 +230,11 @@ __global__ void __launch_bounds__(PK_THREADS) k_pk_rows(const double2 *__restric
       for (int t = 0; t < PK_VALS; ++t) v[t] = 0.0;
       long bb;
       if (c < NH && pk_visit(i, j, c, N, &bb) >= 0) {
-        const float m = (float)sqrt((double)(ab + fac * c * c));
+        const float m = __fsqrt_rn(ab + fac * c * c);  // = (float)sqrt((double)...), see pk_mode
         d = pk_bin(m, te, Nbin);
         if (d >= 0) {
           const double2 z = zbuf[warp][32 * q + lane];
-          const float mu = (float)((1.0 * c) / (double)(N * m));
+          const float mu = __fdiv_rn((float)c, N * m);
           const float P2 = (float)(0.5 * (3. * mu * mu - 1.));
           const double m2 = (double)mu * mu;
           const float mu4 = (float)(m2 * m2), mu6 = (float)(m2 * m2 * m2);
