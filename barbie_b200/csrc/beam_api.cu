@@ -229,8 +229,18 @@ static const double *mapped_host(const double *r2c) {
   return at.type == cudaMemoryTypeHost ? static_cast<const double *>(at.devicePointer) : nullptr;
 }
 
-// Triangle sums of one realization on the plan's own slot.
+// Buffers the kernels read or write as complex128 (double2) must start on a
+// 16-byte boundary.
+static bool aligned16(const void *q) { return ((uintptr_t)q & 15) == 0; }
+
+// Triangle sums of one realization on the plan's own slot. A device r2c
+// buffer must be 16-byte aligned; a page-locked host one that is not is
+// gathered on the host instead of being read in place.
 static int compute_B(beam_gpu_plan *p, const double *r2c, int on_device) {
+  if (on_device && !aligned16(r2c)) {
+    set_detail("the device r2c buffer must be 16-byte aligned");
+    return BEAM_EINVAL;
+  }
   RunSlot *s = p->main;
   s->timed = false;
   s->launches = 0;
@@ -239,7 +249,7 @@ static int compute_B(beam_gpu_plan *p, const double *r2c, int on_device) {
   if (on_device) {
     s->h_src[s->cap] = r2c;
     BEAM_TRY(upload_modes(p, s, 1, false));
-  } else if (const double *mapped = mapped_host(r2c)) {
+  } else if (const double *mapped = aligned16(r2c) ? mapped_host(r2c) : nullptr) {
     BEAM_TRY(gather_mapped(p, s, mapped));
     BEAM_TRY(upload_modes(p, s, 1, true, true));
   } else {
@@ -373,6 +383,10 @@ int beam_gpu_closed_rings(beam_gpu_plan *p, double *rings4, long cap, long *rcou
 int beam_gpu_plane_rings(beam_gpu_plan *p, const double *r2c, int r2c_on_device, const int *planes, const int *rings,
                          int n, double *out, int out_on_device) {
   if (!p || !r2c || !planes || !rings || !out || n < 0) return BEAM_EINVAL;
+  if ((r2c_on_device && !aligned16(r2c)) || (out_on_device && !aligned16(out))) {
+    set_detail("device buffers must be 16-byte aligned");
+    return BEAM_EINVAL;
+  }
   BEAM_CUDA(cudaSetDevice(p->ctx->device));
   return plane_rings(p, r2c, r2c_on_device, planes, rings, n, out, out_on_device);
 }

@@ -475,6 +475,10 @@ extern "C" int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const d
     set_detail("invalid arguments (NN even, 1 <= Nmax <= NN/2, Nr a multiple of 10, device buffers)");
     return BEAM_EINVAL;
   }
+  if (n > 0 && (((uintptr_t)r2c_dev & 15) || ((uintptr_t)out_dev & 15))) {
+    set_detail("device buffers must be 16-byte aligned");
+    return BEAM_EINVAL;
+  }
   if (n > BEAM_NOALLOC_MAX_JOBS) {
     set_detail("more than BEAM_NOALLOC_MAX_JOBS (plane, ring) pairs in one call");
     return BEAM_EINVAL;

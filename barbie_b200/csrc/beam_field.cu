@@ -663,6 +663,14 @@ extern "C" int beam_gpu_field_ingest(beam_gpu_ctx *ctx, long NN, double LL, doub
     set_detail("field ingest: the device cube must be 16-byte aligned");
     return BEAM_EINVAL;
   }
+  if (cube_on_device && r2c_on_device && NN > 0 && NN <= FIELD_MAX_N) {  // the row pass reads one, writes the other
+    const uintptr_t c0 = (uintptr_t)cube, c1 = c0 + sizeof(double) * (size_t)NN * NN * NN;
+    const uintptr_t r0 = (uintptr_t)r2c, r1 = r0 + sizeof(double) * (size_t)NN * NN * (NN + 2);
+    if (c0 < r1 && r0 < c1) {
+      set_detail("field ingest: the cube and the r2c buffer overlap");
+      return BEAM_EINVAL;
+    }
+  }
   FieldRun f;
   int rc = field_begin(ctx, NN, LL, f);
   if (rc != BEAM_OK) return rc;

@@ -348,6 +348,10 @@ extern "C" int beam_gpu_power_multipoles(beam_gpu_ctx *ctx, long NN, double LL, 
     set_detail("power multipoles: NN even in [2, 4096], 1 <= Nbin <= 1024, LL > 0, non-null buffers");
     return BEAM_EINVAL;
   }
+  if (r2c_on_device && ((uintptr_t)r2c & 15)) {  // read as 16-byte complex values
+    set_detail("power multipoles: the device r2c buffer must be 16-byte aligned");
+    return BEAM_EINVAL;
+  }
   BEAM_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   const size_t n_r2c = (size_t)NN * NN * (NN + 2);

@@ -10,7 +10,12 @@
  * Conventions: every call returns BEAM_OK (0) or a negative BEAM_E* code and
  * never exits the process; the caller owns host buffers, the library owns
  * device state; a plan is not re-entrant (one host thread per plan at a time);
- * device waits are bounded and report BEAM_ETIMEDOUT.
+ * device waits are bounded and report BEAM_ETIMEDOUT. Device buffers the
+ * kernels read or write as complex values (r2c buffers, real cubes, plane-ring
+ * outputs) must start on a 16-byte boundary, as cudaMalloc'd and torch
+ * buffers do; a call given one that does not returns BEAM_EINVAL (a
+ * page-locked host r2c buffer off that boundary is gathered on the host
+ * instead of being read in place).
  *
  * Array layouts (all row-major, native-endian):
  *   r2c    double[NN][NN][NN+2]: the FFTW in-place r2c buffer of Delta(k),

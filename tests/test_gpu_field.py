@@ -169,6 +169,24 @@ def test_invalid_sizes_are_rejected(beamlib, ctx):
         beamlib.generate_field(ctx, 12, 1, LL=0.0)
 
 
+def test_overlapping_and_misaligned_device_buffers_are_rejected(beamlib, ctx):
+    """A device cube that overlaps the r2c output, and a device r2c buffer off a
+    16-byte boundary, are refused before any kernel runs."""
+    torch = pytest.importorskip("torch")
+    NN = 16
+    big = torch.zeros(NN * NN * (NN + 2) + NN**3, dtype=torch.float64, device="cuda")
+    out = big[: NN * NN * (NN + 2)].view(NN, NN, NN + 2)
+    cube = big[8: 8 + NN**3].view(NN, NN, NN)  # starts inside the output
+    with pytest.raises(beamlib.BeamError) as e:
+        beamlib.ingest_field(ctx, cube, out=out)
+    assert e.value.code == beamlib.BEAM_EINVAL
+    buf = torch.zeros(NN * NN * (NN + 2) + 1, dtype=torch.float64, device="cuda")
+    odd = buf[1:].view(NN, NN, NN + 2)  # 8 bytes past an aligned start
+    with pytest.raises(beamlib.BeamError) as e:
+        beamlib.power_multipoles(ctx, odd, NN)
+    assert e.value.code == beamlib.BEAM_EINVAL
+
+
 def test_field_cli_matches_reference_generator(tmp_path):
     exe = os.path.join(ROOT, "barbie_b200", "field")
     if not os.path.exists(exe):

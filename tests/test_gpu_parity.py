@@ -126,6 +126,28 @@ def test_runs_are_deterministic_and_device_input_matches(beamlib, ctx):
         assert np.array_equal(a[k], c[k], equal_nan=True), k
 
 
+def test_misaligned_buffers(beamlib, ctx):
+    """A device r2c buffer off a 16-byte boundary is refused (the kernels read
+    it as complex128); a page-locked host one is gathered on the host instead
+    of being read in place, with the same bins."""
+    torch = pytest.importorskip("torch")
+    name = "nn64_cfg1"
+    f = golden_field(name)
+    plan = make_plan(beamlib, ctx, name)
+    a = plan.run(f)
+    n = f.size
+    dev = torch.zeros(n + 1, dtype=torch.float64, device="cuda")
+    dev[1:] = torch.from_numpy(f.ravel()).cuda()
+    with pytest.raises(beamlib.BeamError) as e:
+        plan.run(dev[1:].view(f.shape))
+    assert e.value.code == beamlib.BEAM_EINVAL
+    host = torch.zeros(n + 1, dtype=torch.float64).pin_memory()
+    host[1:] = torch.from_numpy(f.ravel())
+    b = plan.run(host[1:].view(f.shape))
+    for k in a:
+        assert np.array_equal(a[k], b[k], equal_nan=True), k
+
+
 def test_page_locked_host_input_matches_pageable(beamlib, ctx):
     """Page-locked host buffers are read in place by the device (no host gather);
     the bins must be the same bit for bit as from a pageable buffer."""
