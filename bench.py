@@ -613,7 +613,11 @@ def run_reference(args):
                                        f"of one p1 over a window of ring triplets (~{target} accepted triangles); "
                                        f"extrapolated to {ntri} triangles plus the measured cache build "
                                        f"({t_cache:.1f} s) and calCR ({t_calcr:.1f} s)",
-                             "seconds_per_triangle": float(np.median(per_tri)) if per_tri else None},
+                             "seconds_per_triangle": float(np.median(per_tri)) if per_tri else None,
+                             # one reference process for a whole bispectrum (its triangle loop is single-threaded)
+                             "one_process": ({"bispectra_per_hour": 3600.0 / (ntri * float(np.median(per_tri)) + t_cache + t_calcr),
+                                              "seconds_per_bispectrum": ntri * float(np.median(per_tri)) + t_cache + t_calcr}
+                                             if per_tri else None)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
