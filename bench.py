@@ -566,17 +566,21 @@ def run_reference(args):
     ntri = len(tri)
     nproc = max(1, min(cores, 64))
     target = 4000
+    # every window holds min(target, all of its p1's) accepted triangles: a start
+    # too close to the end of the triplet list moves back, so no process runs a
+    # window of a few triangles that start-up would dominate, or of none
     samples = []
+    per_p1 = {p1: np.bincount(tri["rp"][tri["p1"] == p1], minlength=len(rings)) for p1 in np.unique(tri["p1"])}
+    p1s = [p1 for p1 in sorted(per_p1) if per_p1[p1].sum() > 0]
     for k in range(nproc * max(1, args.steps + args.warmup)):
-        p1 = 1 + (7 * k) % 49
-        sel = tri["rp"][tri["p1"] == p1]
-        counts = np.bincount(sel, minlength=len(rings))
-        start = (k * 131) % max(1, len(rings) - 1)
-        acc, end = 0, start
-        while end < len(rings) and acc < target:
-            acc += counts[end]
-            end += 1
-        samples.append((p1, start, end, int(acc)))
+        p1 = int(p1s[(7 * k) % len(p1s)])
+        counts = per_p1[p1]
+        cum = np.concatenate([[0], np.cumsum(counts)])
+        want = min(target, int(cum[-1]))
+        start = (k * 131) % len(rings)
+        start = min(start, int(np.searchsorted(cum, cum[-1] - want, side="right")) - 1)  # suffix holds >= want
+        end = int(np.searchsorted(cum, cum[start] + want, side="left"))
+        samples.append((p1, start, end, int(cum[end] - cum[start])))
 
     def step(k0):
         procs = []
