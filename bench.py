@@ -543,7 +543,8 @@ def run_reference(args):
     field_path = os.path.join(scratch, f"field_N{NN}_R1.txt")
     if not os.path.exists(field_path):
         write_field(field_path, synth_field(NN, realization_seed(1)))
-    env = dict(os.environ, BEAM_REF_NMAX=str(W["Nmax"]), BEAM_REF_NR=str(W["Nr"]))
+    # Nthreads (barbie.c:68, the FFTW threads of its cache build) set to the host's cores
+    env = dict(os.environ, BEAM_REF_NMAX=str(W["Nmax"]), BEAM_REF_NR=str(W["Nr"]), BEAM_REF_NTHREADS=str(cores))
 
     def ref_cmd(p1lo, p1hi, rplo, rphi):
         e = dict(env, BEAM_REF_P1_LO=str(p1lo), BEAM_REF_P1_HI=str(p1hi), BEAM_REF_RP_LO=str(rplo),
