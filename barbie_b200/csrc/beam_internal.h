@@ -60,6 +60,7 @@ constexpr int TRI_PAD = 8;     // zero columns on each side of a mode row (>= TR
 constexpr int TRI_BW = 8, TRI_BLOCKS = 32 / TRI_BW;
 struct TriTile {
   int p1_0[TRI_BLOCKS], p3_0[TRI_BLOCKS];
+  int nblk;  // blocks in use (1..TRI_BLOCKS); the rest repeat block 0 and hold no combos
 };
 
 struct TriChunk {

@@ -278,6 +278,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
           gr.tp1lo = std::min(gr.tp1lo, bp1 * TRI_P1);
           gr.tp1hi = std::max(gr.tp1hi, bp1 * TRI_P1);
         }
+        tl.nblk = nb;
         for (int n = nb; n < TRI_BLOCKS; ++n) {  // unused blocks repeat the first one (no combos)
           tl.p1_0[n] = tl.p1_0[0];
           tl.p3_0[n] = tl.p3_0[0];

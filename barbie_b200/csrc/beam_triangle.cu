@@ -228,6 +228,58 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double av, doubl
       : "d"(av), "d"(bv));
 }
 
+// The pieces of one staged chunk for a tile with NB blocks in use: per group
+// of four triangles, x and z loads and four MMAs per block; at each piece's
+// end, sum += Re(y W) per combo. Blocks NB..3 of a tile hold no combos and
+// are skipped.
+template <int NB>
+__device__ __forceinline__ void dmma_pieces(const double2 *xs, const double2 *zs, const double2 *ys, int px, int pz,
+                                            int Ly, int packed, const int (&ox)[4], const int (&oz)[4],
+                                            const int (&oyb)[4], int t, double (&sum)[4][2]) {
+  const int npc = chunk_npc(packed);
+  int tt = 0;
+  for (int pc = 0; pc < npc; ++pc) {
+    const int len = chunk_len(packed, pc);
+    double wr[NB][2], wi[NB][2];
+#pragma unroll
+    for (int n = 0; n < NB; ++n) wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
+    for (int k0 = 0; k0 < len; k0 += 4) {
+      const bool on = k0 + t < len;
+      const int row = tt + (on ? k0 + t : 0);
+      double2 xv[NB], zv[NB];
+#pragma unroll
+      for (int n = 0; n < NB; ++n) {
+        xv[n] = xs[row * px + ox[n]];
+        zv[n] = zs[row * pz + oz[n]];
+        if (!on) xv[n] = zv[n] = make_double2(0.0, 0.0);
+      }
+      // first the products of the real parts of x, then those of the
+      // imaginary parts: each accumulator's two MMAs are 2 NB apart
+#pragma unroll
+      for (int n = 0; n < NB; ++n) {
+        dmma884(wr[n][0], wr[n][1], xv[n].x, zv[n].x);
+        dmma884(wi[n][0], wi[n][1], xv[n].x, zv[n].y);
+      }
+#pragma unroll
+      for (int n = 0; n < NB; ++n) {
+        dmma884(wr[n][0], wr[n][1], -xv[n].y, zv[n].y);
+        dmma884(wi[n][0], wi[n][1], xv[n].y, zv[n].x);
+      }
+    }
+    tt += len;
+    const double2 *yr = ys + pc * Ly;
+#pragma unroll
+    for (int n = 0; n < NB; ++n)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        int o = oyb[n] - e;
+        o = (unsigned)o < (unsigned)Ly ? o : 0;
+        const double2 y = yr[o];
+        sum[n][e] += fma(y.x, wr[n][e], -y.y * wi[n][e]);
+      }
+  }
+}
+
 // FP64 consumer on the FP64 tensor cores. The warp's tile is four blocks n of
 // 8 planes p1 x 8 planes p3 (TriTile). Per group of four triangles of a
 // piece, every block gets W_n += X_n Z_n^T in complex arithmetic as four real
@@ -242,6 +294,7 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
                                                  int lane, int nch) {
   static_assert(TRI_P1 == 8, "the DMMA consumer tiles 8 planes p1");
   const TriTile tl = a.tiles[it.tile0 + warp];
+  const int nblk = tl.nblk;
   const int g = lane >> 2, t = lane & 3;
   const int px = stage_pitch(it.Lx, true), pz = stage_pitch(it.Lz, true);  // staged row pitches
   const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + g * 32 + 2 * t;
@@ -269,47 +322,11 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
     const double2 *xs = stages + s * a.stage;
     const double2 *zs = xs + TRI_CHUNK * px;
     const double2 *ys = zs + TRI_CHUNK * pz;
-    const int npc = chunk_npc(packed);
-    int tt = 0;
-    for (int pc = 0; pc < npc; ++pc) {
-      const int len = chunk_len(packed, pc);
-      double wr[4][2], wi[4][2];
-#pragma unroll
-      for (int n = 0; n < 4; ++n) wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
-      for (int k0 = 0; k0 < len; k0 += 4) {
-        const bool on = k0 + t < len;
-        const int row = tt + (on ? k0 + t : 0);
-        double2 xv[4], zv[4];
-#pragma unroll
-        for (int n = 0; n < 4; ++n) {
-          xv[n] = xs[row * px + ox[n]];
-          zv[n] = zs[row * pz + oz[n]];
-          if (!on) xv[n] = zv[n] = make_double2(0.0, 0.0);
-        }
-        // first the products of the real parts of x, then those of the
-        // imaginary parts: each accumulator's two MMAs are eight apart
-#pragma unroll
-        for (int n = 0; n < 4; ++n) {
-          dmma884(wr[n][0], wr[n][1], xv[n].x, zv[n].x);
-          dmma884(wi[n][0], wi[n][1], xv[n].x, zv[n].y);
-        }
-#pragma unroll
-        for (int n = 0; n < 4; ++n) {
-          dmma884(wr[n][0], wr[n][1], -xv[n].y, zv[n].y);
-          dmma884(wi[n][0], wi[n][1], xv[n].y, zv[n].x);
-        }
-      }
-      tt += len;
-      const double2 *yr = ys + pc * it.Ly;
-#pragma unroll
-      for (int n = 0; n < 4; ++n)
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          int o = oyb[n] - e;
-          o = (unsigned)o < (unsigned)it.Ly ? o : 0;
-          const double2 y = yr[o];
-          sum[n][e] += fma(y.x, wr[n][e], -y.y * wi[n][e]);
-        }
+    switch (nblk) {  // warp-uniform: the tile's blocks in use
+      case 1: dmma_pieces<1>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
+      case 2: dmma_pieces<2>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
+      case 3: dmma_pieces<3>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
+      default: dmma_pieces<4>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
