@@ -238,16 +238,42 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   for (int u = 0; u < d.n_used; ++u) {
     if (!own[u]) continue;
     int cf = u_cfirst[u], nc = u_ncombo[u];
-    int p3min = 1 << 30;
-    for (int c = cf; c < cf + nc; ++c) p3min = std::min(p3min, -combo_p1[c] - combo_p2[c]);
+    int p3min = 1 << 30, p3max = -(1 << 30), p1max = 0;
+    for (int c = cf; c < cf + nc; ++c) {
+      p3min = std::min(p3min, -combo_p1[c] - combo_p2[c]);
+      p3max = std::max(p3max, -combo_p1[c] - combo_p2[c]);
+      p1max = std::max(p1max, combo_p1[c]);
+    }
+    // Origin of the triplet's block grid: p1 blocks start at 8 b - o1 (o1 in
+    // {0, 4}: the mixed consumer reads a block's planes as aligned float4s),
+    // p3 blocks at p3min - o3 + 8 b (o3 in 0..7). The origin with the fewest
+    // non-empty blocks is kept: fewer MMA cells without a combo.
+    int o1 = 0, o3 = 0;
+    {
+      const int nb1 = (p1max + 4) / TRI_P1 + 1, nb3 = (p3max - p3min + TRI_BW - 1) / TRI_BW + 1;
+      std::vector<char> mark((size_t)nb1 * nb3);
+      int best = 1 << 30;
+      for (int a1 = 0; a1 < TRI_P1; a1 += 4)
+        for (int a3 = 0; a3 < TRI_BW; ++a3) {
+          std::fill(mark.begin(), mark.end(), 0);
+          int nblocks = 0;
+          for (int c = cf; c < cf + nc; ++c) {
+            const int p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
+            char &m = mark[(size_t)((p1 + a1) / TRI_P1) * nb3 + (p3 - p3min + a3) / TRI_BW];
+            nblocks += !m;
+            m = 1;
+          }
+          if (nblocks < best) best = nblocks, o1 = a1, o3 = a3;
+        }
+    }
     std::vector<Slot> slots(nc);
     for (int k = 0; k < nc; ++k) {
       int c = cf + k, p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
-      long long bp1 = p1 / TRI_P1, b3 = (p3 - p3min) / TRI_BW;
+      long long bp1 = (p1 + o1) / TRI_P1, b3 = (p3 - p3min + o3) / TRI_BW;
       // a group is one window of 32 planes p3 over up to TRI_WARPS blocks of
       // planes p1; its non-empty TRI_P1 x TRI_BW blocks are packed four to a tile
-      slots[k] = Slot{(b3 / TRI_BLOCKS) * 1000000 + bp1 / TRI_WARPS, bp1 * 1000000 + b3, p1 % TRI_P1,
-                      (p3 - p3min) % TRI_BW, c};
+      slots[k] = Slot{(b3 / TRI_BLOCKS) * 1000000 + bp1 / TRI_WARPS, bp1 * 1000000 + b3, (p1 + o1) % TRI_P1,
+                      (p3 - p3min + o3) % TRI_BW, c};
     }
     std::sort(slots.begin(), slots.end(), [](const Slot &x, const Slot &y) {
       return x.gkey != y.gkey ? x.gkey < y.gkey : (x.tkey != y.tkey ? x.tkey < y.tkey : x.c < y.c);
@@ -265,8 +291,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
         for (; nb < TRI_BLOCKS && k < slots.size() && slots[k].gkey == gk; ++nb) {
           long long bk = slots[k].tkey;
           int bp1 = (int)(bk / 1000000), b3 = (int)(bk % 1000000);
-          tl.p1_0[nb] = bp1 * TRI_P1;
-          tl.p3_0[nb] = p3min + b3 * TRI_BW;
+          tl.p1_0[nb] = bp1 * TRI_P1 - o1;
+          tl.p3_0[nb] = p3min - o3 + b3 * TRI_BW;
           for (; k < slots.size() && slots[k].tkey == bk && slots[k].gkey == gk; ++k) {
             const Slot &s = slots[k];
             tc[s.a * 32 + nb * TRI_BW + s.lane] = s.c;
@@ -275,8 +301,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
             gr.p2lo = std::min(gr.p2lo, p2); gr.p2hi = std::max(gr.p2hi, p2);
             gr.p3lo = std::min(gr.p3lo, p3); gr.p3hi = std::max(gr.p3hi, p3);
           }
-          gr.tp1lo = std::min(gr.tp1lo, bp1 * TRI_P1);
-          gr.tp1hi = std::max(gr.tp1hi, bp1 * TRI_P1);
+          gr.tp1lo = std::min(gr.tp1lo, tl.p1_0[nb]);
+          gr.tp1hi = std::max(gr.tp1hi, tl.p1_0[nb]);
         }
         tl.nblk = nb;
         for (int n = nb; n < TRI_BLOCKS; ++n) {  // unused blocks repeat the first one (no combos)
