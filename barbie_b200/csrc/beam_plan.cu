@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 #include "beam_internal.h"
 
@@ -234,38 +235,58 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     int r2 = g.rp[3 * p->used_rp[u] + 1];
     k2base[u + 1] = k2base[u] + (p->ring_first[r2 + 1] - p->ring_first[r2]);
   }
+  // Origin of each triplet's block grid: p1 blocks start at 8 b - o1 (o1 in
+  // {0, 4}: the mixed consumer reads a block's planes as aligned float4s),
+  // p3 blocks at p3min - o3 + 8 b (o3 in 0..7). The origin with the fewest
+  // non-empty blocks is kept: fewer MMA cells without a combo. Triplets are
+  // searched in parallel; each block is marked with the number of the origin
+  // being counted, so the marks need no clearing between origins.
+  struct Origin {
+    int p3min, o1, o3;
+  };
+  std::vector<Origin> org(d.n_used, Origin{0, 0, 0});
+  {
+    auto search = [&](int u) {
+      const int cf = u_cfirst[u], nc = u_ncombo[u];
+      int p3min = 1 << 30, p3max = -(1 << 30), p1max = 0;
+      for (int c = cf; c < cf + nc; ++c) {
+        p3min = std::min(p3min, -combo_p1[c] - combo_p2[c]);
+        p3max = std::max(p3max, -combo_p1[c] - combo_p2[c]);
+        p1max = std::max(p1max, combo_p1[c]);
+      }
+      Origin o{p3min, 0, 0};
+      const int nb1 = (p1max + 4) / TRI_P1 + 1, nb3 = (p3max - p3min + TRI_BW - 1) / TRI_BW + 1;
+      std::vector<uint8_t> mark((size_t)nb1 * nb3, 0);
+      int best = 1 << 30;
+      uint8_t stamp = 0;
+      for (int a1 = 0; a1 < TRI_P1; a1 += 4)
+        for (int a3 = 0; a3 < TRI_BW; ++a3) {
+          ++stamp;
+          int nblocks = 0;
+          for (int c = cf; c < cf + nc; ++c) {
+            const int p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
+            uint8_t &m = mark[(size_t)((p1 + a1) / TRI_P1) * nb3 + (p3 - p3min + a3) / TRI_BW];
+            nblocks += (m != stamp);
+            m = stamp;
+          }
+          if (nblocks < best) best = nblocks, o.o1 = a1, o.o3 = a3;
+        }
+      org[u] = o;
+    };
+    const int nt = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (int k = 0; k < nt; ++k)
+      th.emplace_back([&, k]() {
+        for (int u = k; u < d.n_used; u += nt)
+          if (own[u] && u_ncombo[u] > 0) search(u);
+      });
+    for (std::thread &t : th) t.join();
+  }
   // tiles and groups
   for (int u = 0; u < d.n_used; ++u) {
     if (!own[u]) continue;
     int cf = u_cfirst[u], nc = u_ncombo[u];
-    int p3min = 1 << 30, p3max = -(1 << 30), p1max = 0;
-    for (int c = cf; c < cf + nc; ++c) {
-      p3min = std::min(p3min, -combo_p1[c] - combo_p2[c]);
-      p3max = std::max(p3max, -combo_p1[c] - combo_p2[c]);
-      p1max = std::max(p1max, combo_p1[c]);
-    }
-    // Origin of the triplet's block grid: p1 blocks start at 8 b - o1 (o1 in
-    // {0, 4}: the mixed consumer reads a block's planes as aligned float4s),
-    // p3 blocks at p3min - o3 + 8 b (o3 in 0..7). The origin with the fewest
-    // non-empty blocks is kept: fewer MMA cells without a combo.
-    int o1 = 0, o3 = 0;
-    {
-      const int nb1 = (p1max + 4) / TRI_P1 + 1, nb3 = (p3max - p3min + TRI_BW - 1) / TRI_BW + 1;
-      std::vector<char> mark((size_t)nb1 * nb3);
-      int best = 1 << 30;
-      for (int a1 = 0; a1 < TRI_P1; a1 += 4)
-        for (int a3 = 0; a3 < TRI_BW; ++a3) {
-          std::fill(mark.begin(), mark.end(), 0);
-          int nblocks = 0;
-          for (int c = cf; c < cf + nc; ++c) {
-            const int p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
-            char &m = mark[(size_t)((p1 + a1) / TRI_P1) * nb3 + (p3 - p3min + a3) / TRI_BW];
-            nblocks += !m;
-            m = 1;
-          }
-          if (nblocks < best) best = nblocks, o1 = a1, o3 = a3;
-        }
-    }
+    const int p3min = org[u].p3min, o1 = org[u].o1, o3 = org[u].o3;
     std::vector<Slot> slots(nc);
     for (int k = 0; k < nc; ++k) {
       int c = cf + k, p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
