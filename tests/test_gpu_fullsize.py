@@ -1,0 +1,108 @@
+"""The estimator at the full benchmark size, `barbie 384 1 51 1 1` (NN=384,
+Nmax=100, Nr=40, k1 bins 1..51 of width 1), where the oracle estimator would
+take hours: exact geometry against the oracle, and size-independent
+properties of the bins. Needs an sm_100a device.
+
+- Closed ring triplets: the plan's exact integer counts are the oracle's
+  calCR (funcs.c:328-424) at NN=384, Num rounded to NN^2 x an integer.
+- Accepted triangles: the plan's (p1, ring triplet, p2) triangles and their
+  in-plane triangle terms are the oracle's loop (barbie.c:247-298).
+- Per-bin triangle counts: exact, the sum of the oracle's Num/NN^2 over the
+  bin's accepted triangles with B != 0 (barbie.c:355). For a random field
+  B = 0 exactly where a leg is ring 0 on plane 0, and nowhere else;
+  norm[..][0] = NN^2 x count.
+- Cubic scaling: every bin is a sum of triple products of the field's modes,
+  and every rounding step commutes with a power of two, so the field times 2
+  gives bs and out times 8 bit for bit, with norm and counts unchanged, on
+  both precision paths.
+- Mixed path against FP64 on the printed bins (norm[..][0] > 0.1): counts
+  identical; relative error per (l, m, bin) with median <= 1e-6, at least 98%
+  of bins within 1e-5 and none above 1e-2 (bins whose value cancels by
+  1e3-1e4 set the maximum; FP32 inputs cannot reach 1e-5 there)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NN, NMAX, NR, UL, LLK, BW = 384, 100, 40, 51, 1, 1
+
+
+@pytest.fixture(scope="module")
+def ctx(beamlib):
+    c = beamlib.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def plans(beamlib, ctx):
+    p = {prec: beamlib.Plan(ctx, NN, UL, LLK, BW, Nmax=NMAX, Nr=NR, precision=prec) for prec in ("fp64", "mixed")}
+    yield p
+    for plan in p.values():
+        plan.close()
+
+
+@pytest.fixture(scope="module")
+def field(beamlib, ctx):
+    torch = pytest.importorskip("torch")
+    d = torch.empty((NN, NN, NN + 2), dtype=torch.float64, device="cuda")
+    beamlib.generate_field(ctx, NN, beamlib.field_seed(1), out=d)
+    return d
+
+
+@pytest.fixture(scope="module")
+def triples(oracle):
+    rings4 = oracle.closed_rings(NN, NR, NMAX)
+    tri, _ = oracle.enumerate_triples(NN, NMAX, NR, UL, LLK, BW, rings4=rings4)
+    return rings4, tri
+
+
+def test_closed_rings_and_triangles_match_oracle(plans, triples):
+    rings4, tri = triples
+    plan = plans["fp64"]
+    got = plan.closed_rings()
+    assert np.array_equal(got[:, :3], rings4[:, :3])
+    assert np.array_equal(got[:, 3], np.rint(rings4[:, 3] / NN**2) * NN**2)
+    info = plan.info
+    assert info["n_triples"] == len(tri) == 2756382
+    assert info["n_fourier_terms"] == int(np.rint(tri["num"] / NN**2).astype(np.int64).sum())
+
+
+def test_bin_counts_exact(plans, field, triples):
+    _, tri = triples
+    res = plans["fp64"].run(field)
+    # B = 0 exactly, for any field, where a leg is ring 0 on plane 0: the
+    # k = 0 mode is zeroed (funcs.c:104), and ring 0 holds only that pixel
+    dc = np.zeros(len(tri), dtype=bool)
+    for k in "123":
+        dc |= (tri["p" + k] == 0) & (tri["r" + k] == 0)
+    t = tri[~dc]
+    want = np.zeros(res["count"].shape, dtype=np.int64)
+    np.add.at(want, (t["k1_bin"], t["t_bin"], t["mu_bin"]), np.rint(t["num"] / NN**2).astype(np.int64))
+    assert np.array_equal(res["count"], want)
+    assert np.array_equal(res["norm"][..., 0], NN**2 * want.astype(np.float64))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cubic_scaling_is_exact(plans, field, precision):
+    plan = plans[precision]
+    a = plan.run(field)
+    b = plan.run(2.0 * field)
+    assert np.array_equal(b["bs"], 8.0 * a["bs"])
+    assert np.array_equal(b["out"], 8.0 * a["out"], equal_nan=True)
+    assert np.array_equal(b["norm"], a["norm"])
+    assert np.array_equal(b["count"], a["count"])
+    assert np.any(a["count"] > 0)
+
+
+def test_mixed_error_against_fp64(plans, field):
+    f = plans["fp64"].run(field)
+    m = plans["mixed"].run(field)
+    assert np.array_equal(f["count"], m["count"])
+    ok = (f["norm"][..., 0] > 0.1)[..., None] & np.isfinite(f["out"]) & (f["out"] != 0)
+    ok = np.broadcast_to(ok, f["out"].shape)
+    rel = np.abs(m["out"][ok] - f["out"][ok]) / np.abs(f["out"][ok])
+    assert rel.size > 10000
+    assert np.median(rel) <= 1e-6
+    assert np.mean(rel <= 1e-5) >= 0.98
+    assert rel.max() <= 1e-2
