@@ -237,7 +237,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   }
   // Origin of each triplet's block grid: p1 blocks start at 8 b - o1 (o1 in
   // {0, 4}: the mixed consumer reads a block's planes as aligned float4s),
-  // p3 blocks at p3min - o3 + 8 b (o3 in 0..7). The origin with the fewest
+  // p3 blocks at p3min - o3 + 8 b (o3 in 0..7; on the mixed path only those
+  // that put p3 blocks on multiples of 4, for the same reason). The origin with the fewest
   // non-empty blocks is kept: fewer MMA cells without a combo. Triplets are
   // searched in parallel; each block is marked with the number of the origin
   // being counted, so the marks need no clearing between origins.
@@ -259,8 +260,9 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
       std::vector<uint8_t> mark((size_t)nb1 * nb3, 0);
       int best = 1 << 30;
       uint8_t stamp = 0;
+      const int a3first = (A == 4) ? ((p3min % 4) + 4) % 4 : 0, a3step = (A == 4) ? 4 : 1;
       for (int a1 = 0; a1 < TRI_P1; a1 += 4)
-        for (int a3 = 0; a3 < TRI_BW; ++a3) {
+        for (int a3 = a3first; a3 < TRI_BW; a3 += a3step) {
           ++stamp;
           int nblocks = 0;
           for (int c = cf; c < cf + nc; ++c) {
@@ -467,6 +469,10 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
       }
       for (int c = u_cfirst[u]; c < u_cfirst[u] + u_ncombo[u]; ++c) seen[c] = 2;
     }
+    if (A == 4)  // the mixed consumer's float4 reads of x and z
+      for (const TriTile &tl : tiles)
+        for (int n = 0; n < TRI_BLOCKS; ++n)
+          if ((tl.p1_0[n] & 3) || (tl.p3_0[n] & 3)) return set_detail("mixed tile block off a 4-plane boundary"), BEAM_EINVAL;
     for (int32_t c : tile_combo)
       if (c >= 0) {
         if (seen[c]) return set_detail("combo placed twice or outside its shard"), BEAM_EINVAL;
@@ -559,8 +565,8 @@ int build_plan_tables(beam_gpu_plan *p) {
   }
   // bulk copies move whole 16-byte units: rows, their starts and lengths are
   // kept in multiples of A complex values (1 for complex128; 4 for the mixed
-  // path's planar rows, whose real and imaginary parts are copied separately
-  // as floats)
+  // path, whose rows hold blocks of 4 real parts then their 4 imaginary parts,
+  // so a copied segment starts and ends on a whole block)
   const int A = (p->cfg.precision == BEAM_PREC_MIXED) ? 4 : 1;
   auto floorA = [A](int v) { return v - (((v % A) + A) % A); };
   auto ceilA = [A, &floorA](int v) { return floorA(v + A - 1); };

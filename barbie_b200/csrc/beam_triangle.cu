@@ -4,8 +4,8 @@
 // which equals the pixel sum of barbie.c:329-337 (see beam_plan.cu).
 //
 // A CTA takes one work item: n tiles of one ring triplet (r1, r2, r3) over a
-// range of its in-plane triangle list, with n consumer warps (one per tile)
-// and one producer warp. The list is k2-major, cut into pieces (runs of one
+// range of its in-plane triangle list, with one consumer warp per tile (FP64)
+// or per pair of tiles (mixed) and one producer warp. The list is k2-major, cut into pieces (runs of one
 // k2) and chunks (<= TRI_CHUNK triangles, <= TRI_PIECES pieces) described by
 // TriDesc records. The producer streams chunks into a TRI_STAGES-deep ring of
 // shared stages with TMA bulk copies -- per triangle the r1 row of k1 over the
@@ -17,8 +17,8 @@
 // product w(p1, p3) += x_{k1}(p1) z_{k3}(p3) of its tile and at the end of the
 // piece adds Re(y_{k2}(-p1-p3) w(p1, p3)) to the tile's sums. The FP64 path
 // forms the outer products on the FP64 tensor cores (tri_consume_dmma: five
-// 128-bit shared loads per warp for 4096 FMA), the mixed path with FP32 FMA
-// and x broadcast (tri_consume_fma).
+// 128-bit shared loads per warp for 4096 FMA), the mixed path with packed FP32
+// FMA on 4 x 4 patches of combos per lane (tri_consume_fma).
 #include <type_traits>
 
 #include "beam_device.cuh"
@@ -115,10 +115,6 @@ __device__ __forceinline__ double *tri_out(const TriArgs &a, const TriItem &it) 
          a.u_cfirst[it.u];
 }
 
-// FMA consumer (mixed precision). A thread owns the combos (p1_0 + q,
-// p3_0 + lane), q < TRI_P1, of its tile. Over a piece it accumulates
-// w[q] += x_k1(p1_0+q) * z_k3(p3) (4 FMA; x read warp-wide from one address)
-// and at the end of the piece adds Re(y_k2(-p1_0-q-p3) * w[q]) to its sums.
 // Packed FP32 pairs (fma.rn.f32x2: two independent FP32 FMAs in one
 // instruction, sm_100).
 __device__ __forceinline__ unsigned long long f2pack(float lo, float hi) {
@@ -133,19 +129,28 @@ __device__ __forceinline__ void fma2(unsigned long long &d, unsigned long long a
   asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
 }
 
-// Mixed-precision consumer: FP32 FMA with x broadcast. Lane l works on block
-// l / TRI_BW of the tile: plane p3 = p3_0[l / TRI_BW] + l % TRI_BW and the
-// block's 8 planes p1. Staged rows keep the 4-column blocks of the mode rows
-// (4 real parts, then their 4 imaginary parts; mixed_re), so the 8 x values
-// of a triangle are two float4 loads per part and the accumulators of planes
-// (q, q+1) are packed pairs:
-//   Wr(q,q+1) = fma2(Xr(q,q+1), zr, fma2(Xi(q,q+1), -zi, Wr))
-//   Wi(q,q+1) = fma2(Xr(q,q+1), zi, fma2(Xi(q,q+1),  zr, Wi))
-// the same FP32 operations, in the same order, as one FMA pair per plane.
+// Items whose tiles the packed FP32 consumer takes two to a warp (three tiles
+// or more; measured at NN=384, pairing from 4 or 5 tiles was 1.5% and 9%
+// slower); the others get one tile per warp.
+constexpr int TRI_PAIR_MIN = 3;
+__host__ __device__ constexpr bool fma_pairs_tiles(int ntiles) { return ntiles >= TRI_PAIR_MIN; }
+// Consumer warps of a mixed-path CTA with n tiles, and the most of any class.
+__host__ __device__ constexpr int fma_cons_warps(int n) { return fma_pairs_tiles(n) ? (n + 1) / 2 : n; }
+constexpr int fma_max_cons_warps(int n = 1) {
+  return n > TRI_WARPS ? 0 : (fma_cons_warps(n) > fma_max_cons_warps(n + 1) ? fma_cons_warps(n) : fma_max_cons_warps(n + 1));
+}
+
+// Mixed-precision consumer for items of one or two tiles: one tile per warp
+// (the pairing of the consumer below would leave such a CTA a single consumer
+// warp). Lane l works on block l / TRI_BW of the tile: plane
+// p3 = p3_0[l / TRI_BW] + l % TRI_BW and the block's 8 planes p1. A
+// triangle's 8 x values are two float4 loads per part (x read warp-wide from
+// one address per block) and the accumulators of planes (q, q+1) are packed
+// pairs, with the same FP32 operations, in the same order, per combo as below.
 template <typename C>
-__device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem &it, const C *stages, uint64_t *full,
-                                                uint64_t *empty, volatile int *s_fail, int warp, int lane,
-                                                int nch) {
+__device__ __forceinline__ void tri_consume_fma_tile(const TriArgs &a, const TriItem &it, const C *stages,
+                                                     uint64_t *full, uint64_t *empty, volatile int *s_fail, int warp,
+                                                     int lane, int nch) {
   static_assert(std::is_same<C, float2>::value && TRI_P1 == 8, "the packed consumer is the FP32 path, 8 planes p1");
   const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + lane;
   bool any = false;
@@ -217,6 +222,131 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
     const int cidx = tc[q * 32];
     if (cidx >= 0) out[cidx] = sum[q];
   }
+}
+
+// Mixed-precision consumer: FP32 FMA, two tiles per warp. Lane l works on
+// block j = l / 4 of the warp's eight (tile j / 4 of its pair, block j % 4 of
+// that tile) and in it on a 4 x 4 patch of combos: planes
+// p1 = p1_0 + 4 ph + i and p3 = p3_0 + 4 vh + c (i, c < 4; ph = (l >> 1) & 1,
+// vh = l & 1). Staged rows keep the 4-column blocks of the mode rows (4 real
+// parts, then their 4 imaginary parts; mixed_re), and p1_0, p3_0 and the
+// staged columns are multiples of 4, so a triangle's x of the patch's planes
+// p1 is one float4 per part and its z of the planes p3 another. Over a piece
+// the lane accumulates, per combo,
+//   wr = fma(xr, zr, fma(xi, -zi, wr)),  wi = fma(xr, zi, fma(xi, zr, wi))
+// with planes (i, i+1) as packed pairs, and at the end of the piece adds
+// Re(y_k2(-p1-p3) w) to the combo's FP64 sum. Per triangle a warp makes four
+// 128-bit shared loads for 2048 FMA (16 wavefronts, against 18 for 1024 FMA
+// with one plane p3 and 8 planes p1 per lane).
+template <typename C>
+__device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem &it, const C *stages, uint64_t *full,
+                                                uint64_t *empty, volatile int *s_fail, int warp, int lane,
+                                                int nch) {
+  static_assert(std::is_same<C, float2>::value && TRI_P1 == 8 && TRI_BW == 8,
+                "the packed consumer is the FP32 path over 8 x 8 blocks");
+  const int j = lane >> 2, ph = (lane >> 1) & 1, vh = lane & 1;
+  const int tpair = 2 * warp + (j >> 2);           // the lane's tile within the item
+  const bool have = tpair < it.ntiles;             // an odd item's last warp has one tile
+  const int tile = it.tile0 + (have ? tpair : 2 * warp), nb = j & 3;
+  const int P1 = a.tiles[tile].p1_0[nb] + 4 * ph, P3 = a.tiles[tile].p3_0[nb] + 4 * vh;  // patch origin
+  // combo of (i, c): tile_combo[tile][4 ph + i][8 nb + 4 vh + c]
+  const int32_t *tc = a.tile_combo + (size_t)tile * (TRI_P1 * 32) + (4 * ph) * 32 + nb * TRI_BW + 4 * vh;
+  bool any = false;
+  if (have) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) any |= (tc[i * 32 + c] >= 0);
+  }
+  // x reads [ox, ox+4) (whole blocks: always staged); z and y of a lane
+  // without combos read columns that are staged for every item
+  const int ox = P1 + a.colbase - it.colx;
+  const int oz = any ? P3 + a.colbase - it.colz : 0;
+  const int oy0 = any ? -P1 - P3 + a.colbase - it.coly : 6;  // y of (i, c): oy0 - i - c
+  double sum[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) sum[i][c] = 0.0;
+  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
+  for (int ch = 0; ch < nch; ++ch) {
+    const int s = ch % TRI_STAGES;
+    const int packed = packed_next;  // piece layout of this chunk, loaded one chunk ahead
+    if (ch + 1 < nch) packed_next = a.descs[it.ch0 + ch + 1].packed;
+    if (!tri_wait_chunk(a, full, s_fail, ch, lane)) return;
+    const float *xs = reinterpret_cast<const float *>(stages + s * a.stage);
+    const float *zs = xs + 2 * TRI_CHUNK * it.Lx;
+    const float *ys = zs + 2 * TRI_CHUNK * it.Lz;
+    const int npc = chunk_npc(packed);
+    int tt = 0;
+    for (int pc = 0; pc < npc; ++pc) {
+      const int len = chunk_len(packed, pc);
+      unsigned long long wr[4][2], wi[4][2];  // [c][planes (2h, 2h+1)]
+#pragma unroll
+      for (int c = 0; c < 4; ++c) wr[c][0] = wr[c][1] = wi[c][0] = wi[c][1] = 0ull;
+      for (int k = 0; k < len; ++k, ++tt) {
+        const float *xr = xs + 2 * tt * it.Lx + 2 * ox;  // block ox / 4: 4 real, then 4 imaginary parts
+        const float *zr = zs + 2 * tt * it.Lz + 2 * oz;
+        const float4 xre = *reinterpret_cast<const float4 *>(xr);
+        const float4 xim = *reinterpret_cast<const float4 *>(xr + 4);
+        const float4 zre = *reinterpret_cast<const float4 *>(zr);
+        const float4 zim = *reinterpret_cast<const float4 *>(zr + 4);
+        const unsigned long long r0 = f2pack(xre.x, xre.y), r1 = f2pack(xre.z, xre.w);
+        const unsigned long long i0 = f2pack(xim.x, xim.y), i1 = f2pack(xim.z, xim.w);
+        const float zrv[4] = {zre.x, zre.y, zre.z, zre.w}, ziv[4] = {zim.x, zim.y, zim.z, zim.w};
+        // each accumulator's two FMAs in the order above, the second ones of
+        // plane c - 1 after the first ones of plane c (independent work
+        // between dependent FMAs)
+#pragma unroll
+        for (int c = 0; c <= 4; ++c) {
+          if (c < 4) {
+            const unsigned long long ZR = f2pack(zrv[c], zrv[c]), NZI = f2pack(-ziv[c], -ziv[c]);
+            fma2(wr[c][0], i0, NZI);
+            fma2(wi[c][0], i0, ZR);
+            fma2(wr[c][1], i1, NZI);
+            fma2(wi[c][1], i1, ZR);
+          }
+          if (c > 0) {
+            const unsigned long long ZR = f2pack(zrv[c - 1], zrv[c - 1]), ZI = f2pack(ziv[c - 1], ziv[c - 1]);
+            fma2(wr[c - 1][0], r0, ZR);
+            fma2(wi[c - 1][0], r0, ZI);
+            fma2(wr[c - 1][1], r1, ZR);
+            fma2(wi[c - 1][1], r1, ZI);
+          }
+        }
+      }
+      // y of the 7 planes p2 the patch spans: (i, c) reads y[i + c]
+      const float *yr = ys + 2 * pc * it.Ly;
+      float yre[7], yim[7];
+#pragma unroll
+      for (int d = 0; d < 7; ++d) {
+        const float *y = yr + mixed_re(oy0 - d);
+        yre[d] = y[0];
+        yim[d] = y[4];
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          float r0, r1, i0, i1;
+          f2unpack(wr[c][h], r0, r1);
+          f2unpack(wi[c][h], i0, i1);
+          sum[2 * h][c] += (double)fma(yre[2 * h + c], r0, -yim[2 * h + c] * i0);
+          sum[2 * h + 1][c] += (double)fma(yre[2 * h + 1 + c], r1, -yim[2 * h + 1 + c] * i1);
+        }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_addr(&empty[s]));
+  }
+  if (!any) return;
+  double *out = tri_out(a, it);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int cidx = tc[i * 32 + c];
+      if (cidx >= 0) out[cidx] = sum[i][c];
+    }
 }
 
 // D += A * B for one 8x8x4 FP64 tile on the tensor cores (mma.sync m8n8k4,
@@ -341,15 +471,26 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
     }
 }
 
+// Largest CTA of each instantiation (TRI_WARPS tiles plus the producer) and
+// the CTAs per SM its register budget is sized for.
 template <typename C>
-__global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a) {
+struct TriBounds {
+  static constexpr int threads = 32 * (TRI_WARPS + 1), blocks = 2;
+};
+template <>
+struct TriBounds<float2> {
+  static constexpr int threads = 32 * (fma_max_cons_warps() + 1), blocks = 3;
+};
+
+template <typename C>
+__global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks) k_triangle(TriArgs a) {
   typedef typename TriAcc<C>::t acc_t;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[TRI_STAGES], empty[TRI_STAGES];
   __shared__ volatile int s_fail;
   const TriItem it = a.items[blockIdx.x];  // realization blockIdx.y
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ncons = (blockDim.x >> 5) - 1;  // consumer warps == it.ntiles; warp ncons produces
+  const int ncons = (blockDim.x >> 5) - 1;  // consumer warps (cons_warps); warp ncons produces
   if (tid == 0) {
     for (int s = 0; s < TRI_STAGES; ++s) {
       mbar_init(smem_addr(&full[s]), 1);
@@ -394,6 +535,8 @@ __global__ void __launch_bounds__(32 * (TRI_WARPS + 1), 2) k_triangle(TriArgs a)
   // -------------------------------------------------------------- consumer
   if constexpr (std::is_same<C, double2>::value)
     tri_consume_dmma(a, it, stages, full, empty, &s_fail, warp, lane, nch);
+  else if (!fma_pairs_tiles(it.ntiles))
+    tri_consume_fma_tile<C>(a, it, stages, full, empty, &s_fail, warp, lane, nch);
   else
     tri_consume_fma<C>(a, it, stages, full, empty, &s_fail, warp, lane, nch);
 }
@@ -415,6 +558,14 @@ __global__ void k_reduce(long long n_combo, const int32_t *__restrict__ combo_u,
   double s = 0.0;
   for (int k = 0; k < ns; ++k) s += p[(long long)k * nc];
   B[combo_out[c]] = nn2 * s;
+}
+
+// Consumer warps of a CTA with n tiles: one per tile on the FP64 tensor
+// cores and for the FP32 consumer of one or two tiles, one per pair of tiles
+// for the packed FP32 consumer of more.
+template <typename C>
+static int cons_warps(int n) {
+  return std::is_same<C, double2>::value ? n : fma_cons_warps(n);
 }
 
 template <typename C>
@@ -441,7 +592,7 @@ int triangle_init_attributes(size_t smem_optin) {
   return BEAM_OK;
 }
 
-// One launch per tile count n (CTAs of n consumer warps + 1 producer warp), on
+// One launch per tile count n (CTAs of cons_warps(n) consumer warps + 1 producer warp), on
 // side streams forked from and joined back into the slot's stream, so the
 // launches overlap. Each launch covers its class's items for all realizations
 // (blockIdx.y).
@@ -458,7 +609,8 @@ static int launch_classes(beam_gpu_plan *p, RunSlot *s, TriArgs a) {
     TriArgs b = a;
     b.items = d.items + first;
     b.stage = d.class_stage[n];
-    k_triangle<C><<<dim3((unsigned)count, (unsigned)a.nreal), 32 * (n + 1), tri_smem<C>(b.stage, n), st>>>(b);
+    k_triangle<C><<<dim3((unsigned)count, (unsigned)a.nreal), 32 * (cons_warps<C>(n) + 1), tri_smem<C>(b.stage, n),
+                    st>>>(b);
     BEAM_CUDA(cudaGetLastError());
     s->launches++;
     BEAM_CUDA(cudaEventRecord(ln->join[n - 1], st));
