@@ -64,6 +64,41 @@ def synth_field(NN: int, seed: int, LL: float = DEFAULT_LL, quad: float = DEFAUL
     return buf
 
 
+def synth_field_torch(NN: int, seed: int, device="cuda", LL: float = DEFAULT_LL, quad: float = DEFAULT_QUAD,
+                      kaiser: float = DEFAULT_KAISER, slope: float = DEFAULT_SLOPE):
+    """The same recipe as synth_field with torch (on a GPU, milliseconds per
+    field at NN=256 instead of seconds): a torch tensor of shape (NN, NN, NN+2),
+    float64, on `device`. The white noise comes from torch's generator seeded
+    with `seed`, so the fields differ from synth_field's for the same seed but
+    share their spectrum, non-Gaussian term and distortion."""
+    import torch
+    if NN <= 0 or NN % 2:
+        raise ValueError("NN must be a positive even integer")
+    dev = torch.device(device)
+    g = torch.Generator(device=dev).manual_seed(int(seed))
+    W = torch.fft.rfftn(torch.randn((NN, NN, NN), dtype=torch.float64, device=dev, generator=g))
+    kx = 2.0 * np.pi * torch.fft.fftfreq(NN, d=LL, dtype=torch.float64, device=dev)
+    kz = 2.0 * np.pi * torch.fft.rfftfreq(NN, d=LL, dtype=torch.float64, device=dev)
+    k2 = kx[:, None, None] ** 2 + kx[None, :, None] ** 2 + kz[None, None, :] ** 2
+    k = torch.sqrt(k2)
+    kc = 0.5 * np.pi / LL
+    pos = k > 0
+    amp = torch.where(pos, torch.where(pos, k, 1.0) ** (0.5 * slope) * torch.exp(-0.5 * (k / kc) ** 2),
+                      torch.zeros_like(k))
+    delta = torch.fft.irfftn(W * amp, s=(NN, NN, NN))
+    del W, amp
+    delta /= torch.sqrt(torch.mean(delta * delta))
+    d2 = delta * delta
+    delta += quad * (d2 - d2.mean())
+    del d2
+    D = torch.fft.rfftn(delta) * LL ** 3
+    del delta
+    mu2 = torch.where(pos, kz[None, None, :] ** 2 / torch.where(pos, k2, 1.0), torch.zeros_like(k2))
+    D *= 1.0 + kaiser * mu2
+    D[0, 0, 0] = 0.0
+    return torch.view_as_real(D).reshape(NN, NN, NN + 2).contiguous()
+
+
 def write_field(path: str, buf: np.ndarray) -> None:
     """Write the buffer as the reference's raw native-double field file."""
     np.ascontiguousarray(buf, dtype=np.float64).tofile(path)

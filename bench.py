@@ -61,7 +61,7 @@ def parse_args():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default work decomposition and FFT tiles (no beam_gpu_*_autotune)")
     ap.add_argument("--serve-jobs", type=int, default=40, help="jobs per precision in the serving stream")
-    ap.add_argument("--batch-pool", type=int, default=8, help="distinct fields cycled over the batch")
+    ap.add_argument("--batch-pool", type=int, default=64, help="distinct fields cycled over the batch")
     return ap.parse_args()
 
 
@@ -328,13 +328,18 @@ def run_batched(ctx, args):
     timed end to end on the host clock, against the same fields one
     beam_gpu_run call at a time."""
     from barbie_b200 import beam
-    from barbie_b200.synth import realization_seed, synth_field
+    from barbie_b200.synth import realization_seed, synth_field_torch
     B = BATCH
-    pool = [synth_field(B["NN"], realization_seed(r)) for r in range(1, args.batch_pool + 1)]
+    # the field recipe on the GPU (milliseconds per field), copied to host memory
+    dev = f"cuda:{ctx.device}"
+    pool = [synth_field_torch(B["NN"], realization_seed(r), device=dev).cpu().numpy()
+            for r in range(1, args.batch_pool + 1)]
     fields = [pool[i % len(pool)] for i in range(B["realizations"])]
     out = {"workload": f"{B['realizations']} realizations at NN={B['NN']}, Nmax={B['Nmax']}, Nr={B['Nr']}, "
                        f"k1 bins 1..{B['UL_k1']} width 1",
-           "fields": f"{len(pool)} distinct seeded fields cycled over the {B['realizations']} realizations",
+           "fields": (f"{len(pool)} distinct seeded fields (seeds 100020+146r, r=1..{len(pool)}; the field recipe "
+                      f"run with torch on the GPU, then held in host memory)"
+                      + (f", cycled over the {B['realizations']} realizations" if len(pool) < B["realizations"] else "")),
            "timing": "host wall clock around each call (host gather, H2D, kernels, D2H of the bins)"}
     for prec in ("mixed", "fp64"):
         plan = beam.Plan(ctx, B["NN"], B["UL_k1"], B["LL_k1"], B["BW_k1"], Nmax=B["Nmax"], Nr=B["Nr"],
