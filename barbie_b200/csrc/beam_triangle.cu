@@ -262,7 +262,9 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
   // without combos read columns that are staged for every item
   const int ox = P1 + a.colbase - it.colx;
   const int oz = any ? P3 + a.colbase - it.colz : 0;
-  const int oy0 = any ? -P1 - P3 + a.colbase - it.coly : 6;  // y of (i, c): oy0 - i - c
+  // y of (i, c): column oy0 - i - c; oy0 is a multiple of 4 (P1, P3, colbase
+  // and coly are), and a lane without combos reads columns 2..8
+  const int oy0 = any ? -P1 - P3 + a.colbase - it.coly : 8;
   double sum[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
@@ -315,14 +317,23 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
           }
         }
       }
-      // y of the 7 planes p2 the patch spans: (i, c) reads y[i + c]
+      // y of the 7 planes p2 the patch spans, (i, c) reading y[i + c] =
+      // column oy0 - i - c: column oy0 is the first of its 4-column block,
+      // oy0 - 4 .. oy0 - 1 the whole block before it, oy0 - 6 and oy0 - 5
+      // the last two of the block before that
       const float *yr = ys + 2 * pc * it.Ly;
       float yre[7], yim[7];
-#pragma unroll
-      for (int d = 0; d < 7; ++d) {
-        const float *y = yr + mixed_re(oy0 - d);
-        yre[d] = y[0];
-        yim[d] = y[4];
+      {
+        const float4 b1r = *reinterpret_cast<const float4 *>(yr + 2 * (oy0 - 4));
+        const float4 b1i = *reinterpret_cast<const float4 *>(yr + 2 * (oy0 - 4) + 4);
+        const float2 b0r = *reinterpret_cast<const float2 *>(yr + 2 * (oy0 - 8) + 2);
+        const float2 b0i = *reinterpret_cast<const float2 *>(yr + 2 * (oy0 - 8) + 6);
+        yre[0] = yr[2 * oy0];
+        yim[0] = yr[2 * oy0 + 4];
+        yre[1] = b1r.w, yre[2] = b1r.z, yre[3] = b1r.y, yre[4] = b1r.x;
+        yim[1] = b1i.w, yim[2] = b1i.z, yim[3] = b1i.y, yim[4] = b1i.x;
+        yre[5] = b0r.y, yre[6] = b0r.x;
+        yim[5] = b0i.y, yim[6] = b0i.x;
       }
 #pragma unroll
       for (int c = 0; c < 4; ++c)
