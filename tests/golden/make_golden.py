@@ -56,13 +56,13 @@ FIELD_CASES = {"n16_r1": (16, 1), "n24_r3": (24, 3)}
 
 # name: (NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, realization)
 CASES = {
-    # BASELINE config 1 (CPU-runnable): NN=64, Nmax=16, Nr=10, bins 1..11 width 1
+    # the CPU-runnable case: NN=64, Nmax=16, Nr=10, bins 1..11 width 1
     "nn64_cfg1": (64, 16, 10, 11, 1, 1, 1),
     # same geometry, other realization, wider bins and an offset k1 range
     "nn64_bw2": (64, 16, 10, 13, 3, 2, 2),
     # radix-3 grid, 20 rings in two blocks of widths 1 and 2
     "nn96_r20": (96, 32, 20, 21, 1, 1, 3),
-    # NN=256, Nmax=64, Nr=30, bins 1..31 width 1
+    # the drop-in comparison case: NN=256, Nmax=64, Nr=30, bins 1..31 width 1
     "nn256_cfg2": (256, 64, 30, 31, 1, 1, 1),
 }
 
