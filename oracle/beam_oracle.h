@@ -2,8 +2,8 @@
  * (reference: barbie.c + funcs.c of sukhdeepsinghgill/BARBIE).
  *
  * TEST INFRASTRUCTURE ONLY. The pytest suite, the smoke entry point and the
- * benchmark's CPU-baseline leg use it as the checker; the GPU product library
- * (libbeam_gpu.so) never links or calls it.
+ * benchmark's CPU-baseline leg compare against it or time it; the GPU product
+ * library (libbeam_gpu.so) never links or calls it.
  *
  * Parity of this restatement is pinned against the reference program itself,
  * compiled from its own sources with an FFTW-API shim (oracle/Makefile), on the

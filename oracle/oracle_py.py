@@ -1,8 +1,8 @@
 """ctypes binding of the oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
-the CPU-baseline leg of ``bench.py`` as the checker. The GPU product path never
-imports this module.
+the CPU-baseline leg of ``bench.py``, to compare against or to time. The GPU
+product path never imports this module.
 
 Each wrapper names the reference lines (barbie.c / funcs.c of
 sukhdeepsinghgill/BARBIE) its C function restates.
