@@ -100,6 +100,27 @@ def test_pixel_method_matches_triangle_method(beamlib, ctx, name):
     assert np.array_equal(a["count"], b["count"])
 
 
+def test_serving_geometry_matches_oracle(beamlib, ctx, oracle):
+    """A job shape of the served mix: NN=128 with Nr=20 rings to Nmax=40 and k1
+    bins 1..41 of width 2 (neither in the golden cases), FP64 at 1e-10 of the
+    oracle per printed bin with exact counts, and the mixed path's counts."""
+    from barbie_b200.synth import realization_seed, synth_field
+    NN, Nmax, Nr, UL, LL, BW = 128, 40, 20, 41, 1, 2
+    f = synth_field(NN, realization_seed(7))
+    want = oracle.estimate(f, NN, Nmax, Nr, UL, LL, BW)
+    res = beamlib.Plan(ctx, NN, UL, LL, BW, Nmax=Nmax, Nr=Nr).run(f)
+    ok = want["norm"][..., 0] > 0.1
+    assert np.array_equal(res["norm"][..., 0] > 0.1, ok) and ok.sum() > 100
+    for key, wkey in (("bs", "bs"), ("norm", "norm"), ("out", "out")):
+        a, b = res[key][ok], want[wkey][ok]
+        fin = np.isfinite(b)
+        assert np.array_equal(np.isfinite(a), fin), key
+        assert np.all(np.abs(a[fin] - b[fin]) <= 1e-10 * np.abs(b[fin]) + 1e-300), key
+    assert np.array_equal(res["count"], want["counts"])
+    mix = beamlib.Plan(ctx, NN, UL, LL, BW, Nmax=Nmax, Nr=Nr, precision="mixed").run(f)
+    assert np.array_equal(mix["count"], want["counts"])
+
+
 def test_mixed_precision_error_is_bounded(beamlib, ctx):
     name = "nn96_r20"
     f = golden_field(name)
