@@ -384,15 +384,18 @@ __device__ __forceinline__ void dmma_pieces(const double2 *xs, const double2 *zs
     double wr[NB][2], wi[NB][2];
 #pragma unroll
     for (int n = 0; n < NB; ++n) wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
-    for (int k0 = 0; k0 < len; k0 += 4) {
-      const bool on = k0 + t < len;
+    // one group of four triangles; only a piece's last group can be partial
+    // (CHECK: its rows past the piece's end are zeroed)
+    auto group = [&](int k0, auto check) {
+      constexpr bool CHECK = decltype(check)::value;
+      const bool on = !CHECK || k0 + t < len;
       const int row = tt + (on ? k0 + t : 0);
       double2 xv[NB], zv[NB];
 #pragma unroll
       for (int n = 0; n < NB; ++n) {
         xv[n] = xs[row * px + ox[n]];
         zv[n] = zs[row * pz + oz[n]];
-        if (!on) xv[n] = zv[n] = make_double2(0.0, 0.0);
+        if (CHECK && !on) xv[n] = zv[n] = make_double2(0.0, 0.0);
       }
       // first the products of the real parts of x, then those of the
       // imaginary parts: each accumulator's two MMAs are 2 NB apart
@@ -406,7 +409,10 @@ __device__ __forceinline__ void dmma_pieces(const double2 *xs, const double2 *zs
         dmma884(wr[n][0], wr[n][1], -xv[n].y, zv[n].y);
         dmma884(wi[n][0], wi[n][1], xv[n].y, zv[n].x);
       }
-    }
+    };
+    int k0 = 0;
+    for (; k0 + 4 <= len; k0 += 4) group(k0, std::false_type{});
+    if (k0 < len) group(k0, std::true_type{});
     tt += len;
     const double2 *yr = ys + pc * Ly;
 #pragma unroll
