@@ -276,15 +276,16 @@ def run_ours(args):
                  "speedup_vs_fp64": (sum(times) / sum(mt)), **mixed_errors(ref, got)}
         plan_m.close()
 
-    # roofline of the dominant kernel (triangle sums, FP64 pipe)
+    # roofline of the dominant kernel (triangle sums on the FP64 tensor pipe, mma.sync m8n8k4.f64)
     peak = measured_fp64_peak(torch, dev)
     tri_avg = float(np.mean(tri_ms))
     flops = 10.0 * info["n_fourier_terms"]  # complex a*b (6) + Re(ab*c) (3) + accumulate (1)
     achieved = flops / (tri_avg / 1e3) / 1e12
-    roofline = {"kernel": "k_triangle<double2>", "bound": "fp64", "achieved": achieved, "peak": peak,
+    roofline = {"kernel": "k_triangle<double2>", "bound": "tensor", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": profile_traffic("k_triangle"),
                 "flops_per_launch": flops, "launch_ms": tri_avg,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
+                "peak_source": ("FP64 tensor pipe: cuBLAS DGEMM 8192^3 measured in this run "
+                                "(MEASURED_PEAKS.json has no FP64 figure)"),
                 "pixel_equivalent_tflops": 4.0 * info["n_triples"] * W["NN"] ** 2 / (tri_avg / 1e3) / 1e12}
 
     cpu = None
@@ -437,7 +438,7 @@ def run_field(ctx, plan, stream, args):
             "timing": "median of CUDA-event times around each call on the library stream",
             "autotune": tiles,
             "power_multipoles": {"ms": pk_ms, "bins": 10, "roofline": {
-                "kernel": "k_pk_planes + k_pk_total", "bound": "hbm", "achieved": pk_bytes / (pk_ms / 1e3) / 1e9,
+                "kernel": "k_pk_rows + k_pk_total", "bound": "hbm", "achieved": pk_bytes / (pk_ms / 1e3) / 1e9,
                 "peak": peak[0], "unit": "GB/s", "frac": pk_bytes / (pk_ms / 1e3) / 1e9 / peak[0],
                 "bytes": pk_bytes}}}
 
