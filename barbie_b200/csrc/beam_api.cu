@@ -137,9 +137,9 @@ int beam_gpu_plan_create(beam_gpu_ctx *ctx, const beam_cfg *cfg, beam_gpu_plan *
   if (rc == BEAM_EBOUNDS) set_detail("a triangle's (k1, t, mu) bin falls outside the bin arrays");
   if (rc == BEAM_EINVAL) set_detail("invalid configuration (NN even, Nmax <= NN/2, Nr a multiple of 10, "
                                     "BW_k1 > 0 dividing UL_k1 - LL_k1 > 0)");
-  if (rc == BEAM_OK) rc = build_plan_tables(p);
-  if (rc == BEAM_OK) rc = slot_create(p, 1, &ctx->lane, &p->main);
-  if (rc == BEAM_OK && pixel_method(p)) rc = build_pixel_path(p);
+  if (rc == BEAM_OK) rc = host_guard([&] { return build_plan_tables(p); });
+  if (rc == BEAM_OK) rc = host_guard([&] { return slot_create(p, 1, &ctx->lane, &p->main); });
+  if (rc == BEAM_OK && pixel_method(p)) rc = host_guard([&] { return build_pixel_path(p); });
   if (rc != BEAM_OK) {
     beam_gpu_plan_destroy(p);
     return rc;
@@ -211,11 +211,9 @@ static void gather_one(const beam_gpu_plan *p, RunSlot *s, const double *r2c) {
     gather_host(p, s, 0, r2c);
     return;
   }
-  std::vector<std::thread> th;
-  for (int k = 1; k < nt; ++k)
-    th.emplace_back([=]() { gather_host(p, s, 0, r2c, (int)((long long)nm * k / nt), (int)((long long)nm * (k + 1) / nt)); });
-  gather_host(p, s, 0, r2c, 0, nm / nt);
-  for (std::thread &t : th) t.join();
+  host_parallel(nt, [=](int k) {
+    gather_host(p, s, 0, r2c, (int)((long long)nm * k / nt), (int)((long long)nm * (k + 1) / nt));
+  });
 }
 
 // Device-side address of a page-locked host buffer (cudaHostAlloc'd or
@@ -282,12 +280,9 @@ static void gather_batch(const beam_gpu_plan *p, RunSlot *s, const double *const
     for (int r = 0; r < n; ++r) gather_host(p, s, r, r2c[r]);
     return;
   }
-  std::vector<std::thread> th;
-  for (int k = 0; k < nt; ++k)
-    th.emplace_back([=]() {
-      for (int r = k; r < n; r += nt) gather_host(p, s, r, r2c[r]);
-    });
-  for (std::thread &t : th) t.join();
+  host_parallel(nt, [=](int k) {
+    for (int r = k; r < n; r += nt) gather_host(p, s, r, r2c[r]);
+  });
 }
 
 int beam_gpu_run_batch_ex(beam_gpu_plan *p, const double *const *r2c, int n, beam_result *res, int batch) {

@@ -4,8 +4,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <string>
+#include <exception>
 #include <map>
+#include <new>
+#include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -18,6 +21,38 @@ struct PixelPath;  // FFT-path state (beam_fft.cu)
 
 // Thread-local detail text for the last failure (beam_gpu_last_error_detail).
 void set_detail(const std::string &s);
+
+// Host-side C++ failures (allocation, thread start) as an error code, so no
+// exception leaves a C entry point.
+template <typename F>
+int host_guard(F &&f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc &) {
+    set_detail("host memory allocation failed");
+    return BEAM_ENOMEM;
+  } catch (const std::exception &e) {
+    set_detail(std::string("host: ") + e.what());
+    return BEAM_ENOMEM;
+  }
+}
+
+// fn(k) for k = 0 .. n-1 on up to n - 1 extra host threads. k = 0, and every k
+// whose thread could not be started, run on the calling thread, so a failed
+// thread start costs time, not an exception.
+template <typename F>
+void host_parallel(int n, const F &fn) {
+  std::vector<std::thread> th;
+  int started = 1;
+  try {
+    th.reserve(n > 1 ? n - 1 : 0);
+    for (; started < n; ++started) th.emplace_back(fn, started);
+  } catch (...) {
+  }
+  fn(0);
+  for (int k = started; k < n; ++k) fn(k);
+  for (std::thread &t : th) t.join();
+}
 
 // Evaluate a CUDA runtime call; on failure record the detail and return BEAM_ECUDA
 // (or BEAM_EDEVMEM for allocation failures) from the enclosing function.

@@ -276,13 +276,10 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
       org[u] = o;
     };
     const int nt = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> th;
-    for (int k = 0; k < nt; ++k)
-      th.emplace_back([&, k]() {
-        for (int u = k; u < d.n_used; u += nt)
-          if (own[u] && u_ncombo[u] > 0) search(u);
-      });
-    for (std::thread &t : th) t.join();
+    host_parallel(nt, [&](int k) {
+      for (int u = k; u < d.n_used; u += nt)
+        if (own[u] && u_ncombo[u] > 0) search(u);
+    });
   }
   // tiles and groups
   for (int u = 0; u < d.n_used; ++u) {

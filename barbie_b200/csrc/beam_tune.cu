@@ -74,8 +74,8 @@ static int rebuild(beam_gpu_plan *p, long long tau0, double balance) {
   p->device_bytes = 0;
   p->tau0 = tau0;
   p->balance = balance;
-  int rc = build_plan_tables(p);
-  if (rc == BEAM_OK) rc = slot_create(p, 1, &p->ctx->lane, &p->main);
+  int rc = host_guard([&] { return build_plan_tables(p); });
+  if (rc == BEAM_OK) rc = host_guard([&] { return slot_create(p, 1, &p->ctx->lane, &p->main); });
   return rc;
 }
 
