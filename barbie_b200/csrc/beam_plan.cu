@@ -121,38 +121,51 @@ static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, con
   int rc = BEAM_OK;
   std::vector<int> cnt(k2total);
   std::vector<long long> offs(k2total);
-  BEAM_CUDA(cudaMalloc(&d_refs, sizeof(TripletRef) * refs.size()));
-  BEAM_CUDA(cudaMalloc(&d_cnt, sizeof(int) * k2total));
-  BEAM_CUDA(cudaMemcpyAsync(d_refs, refs.data(), sizeof(TripletRef) * refs.size(), cudaMemcpyHostToDevice, s));
-  for (size_t y0 = 0; y0 < refs.size(); y0 += 65535) {
-    dim3 grid((max_n2 + 127) / 128, (unsigned)std::min<size_t>(65535, refs.size() - y0));
-    k_tri_count<<<grid, 128, 0, s>>>(d_refs + y0, d_mode_ij, d_ringmap, (int)g.NN, d_cnt);
-  }
-  BEAM_CUDA(cudaGetLastError());
-  BEAM_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * k2total, cudaMemcpyDeviceToHost, s));
-  BEAM_CUDA(cudaStreamSynchronize(s));
-  long long run = 0;
-  for (size_t u = 0; u < refs.size(); ++u) {
-    tri_first[u] = run;
-    for (int k = 0; k < refs[u].n2; ++k) {
-      offs[refs[u].k2base + k] = run;
-      run += cnt[refs[u].k2base + k];
+  // a failed CUDA call records its error and skips the rest; the buffers are
+  // freed on every path
+  auto cuda_ok = [&](cudaError_t e, const char *what) {
+    if (rc == BEAM_OK && e != cudaSuccess) {
+      set_detail(std::string(what) + ": " + cudaGetErrorString(e));
+      rc = BEAM_ECUDA;
     }
+    return rc == BEAM_OK;
+  };
+  if (cuda_ok(cudaMalloc(&d_refs, sizeof(TripletRef) * refs.size()), "cudaMalloc(triplets)") &&
+      cuda_ok(cudaMalloc(&d_cnt, sizeof(int) * k2total), "cudaMalloc(counts)") &&
+      cuda_ok(cudaMemcpyAsync(d_refs, refs.data(), sizeof(TripletRef) * refs.size(), cudaMemcpyHostToDevice, s),
+              "cudaMemcpyAsync(triplets)")) {
+    for (size_t y0 = 0; y0 < refs.size(); y0 += 65535) {
+      dim3 grid((max_n2 + 127) / 128, (unsigned)std::min<size_t>(65535, refs.size() - y0));
+      k_tri_count<<<grid, 128, 0, s>>>(d_refs + y0, d_mode_ij, d_ringmap, (int)g.NN, d_cnt);
+    }
+    if (cuda_ok(cudaGetLastError(), "k_tri_count") &&
+        cuda_ok(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * k2total, cudaMemcpyDeviceToHost, s),
+                "cudaMemcpyAsync(counts)"))
+      cuda_ok(cudaStreamSynchronize(s), "k_tri_count");
   }
-  tri_first[refs.size()] = run;
-  if (n_terms) *n_terms = run;
-  if (k2cnt) *k2cnt = cnt;
-  if (d_list) {
-    rc = dev_alloc(p, d_list, (size_t)run);
-    if (rc == BEAM_OK) {
-      BEAM_CUDA(cudaMalloc(&d_offs, sizeof(long long) * k2total));
-      BEAM_CUDA(cudaMemcpyAsync(d_offs, offs.data(), sizeof(long long) * k2total, cudaMemcpyHostToDevice, s));
-      for (size_t y0 = 0; y0 < refs.size(); y0 += 65535) {
-        dim3 grid((max_n2 + 127) / 128, (unsigned)std::min<size_t>(65535, refs.size() - y0));
-        k_tri_write<<<grid, 128, 0, s>>>(d_refs + y0, d_mode_ij, d_ringmap, d_pixlocal, (int)g.NN, d_offs, *d_list);
+  if (rc == BEAM_OK) {
+    long long run = 0;
+    for (size_t u = 0; u < refs.size(); ++u) {
+      tri_first[u] = run;
+      for (int k = 0; k < refs[u].n2; ++k) {
+        offs[refs[u].k2base + k] = run;
+        run += cnt[refs[u].k2base + k];
       }
-      BEAM_CUDA(cudaGetLastError());
-      BEAM_CUDA(cudaStreamSynchronize(s));
+    }
+    tri_first[refs.size()] = run;
+    if (n_terms) *n_terms = run;
+    if (k2cnt) *k2cnt = cnt;
+    if (d_list) {
+      rc = dev_alloc(p, d_list, (size_t)run);
+      if (rc == BEAM_OK && cuda_ok(cudaMalloc(&d_offs, sizeof(long long) * k2total), "cudaMalloc(offsets)") &&
+          cuda_ok(cudaMemcpyAsync(d_offs, offs.data(), sizeof(long long) * k2total, cudaMemcpyHostToDevice, s),
+                  "cudaMemcpyAsync(offsets)")) {
+        for (size_t y0 = 0; y0 < refs.size(); y0 += 65535) {
+          dim3 grid((max_n2 + 127) / 128, (unsigned)std::min<size_t>(65535, refs.size() - y0));
+          k_tri_write<<<grid, 128, 0, s>>>(d_refs + y0, d_mode_ij, d_ringmap, d_pixlocal, (int)g.NN, d_offs, *d_list);
+        }
+        if (cuda_ok(cudaGetLastError(), "k_tri_write")) cuda_ok(cudaStreamSynchronize(s), "k_tri_write");
+      }
     }
   }
   cudaFree(d_refs);
