@@ -217,21 +217,32 @@ int plane_rings(beam_gpu_plan *p, const double *r2c, int on_device, const int *p
   const size_t n2 = (size_t)g.NN * g.NN, rbytes = sizeof(double) * (size_t)g.NN * g.NN * (g.NN + 2);
   double *d_r2c = nullptr, *d_out = nullptr;
   int32_t *d_jobs = nullptr;
-  if (!on_device) {
-    BEAM_CUDA(cudaMalloc(&d_r2c, rbytes));
-    BEAM_CUDA(cudaMemcpyAsync(d_r2c, r2c, rbytes, cudaMemcpyHostToDevice, s));
-  }
-  if (!out_on_device) BEAM_CUDA(cudaMalloc(&d_out, sizeof(double) * 2 * n2 * std::max(1, n)));
-  BEAM_CUDA(cudaMalloc(&d_jobs, sizeof(int32_t) * 2 * std::max(1, n)));
-  BEAM_CUDA(cudaMemcpyAsync(d_jobs, planes, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-  BEAM_CUDA(cudaMemcpyAsync(d_jobs + n, rings, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
-  size_t before = p->device_bytes;
-  rc = launch_dft<double2>(p, px, on_device ? r2c : d_r2c, d_jobs, d_jobs + n, n,
-                           (double2 *)(out_on_device ? out : d_out), (long long)n2);
-  p->device_bytes = before;
+  // a failed CUDA call records its error and skips the rest; the temporary
+  // buffers are freed on every path
+  auto cuda_ok = [&](cudaError_t e, const char *what) {
+    if (rc == BEAM_OK && e != cudaSuccess) {
+      set_detail(std::string(what) + ": " + cudaGetErrorString(e));
+      rc = BEAM_ECUDA;
+    }
+    return rc == BEAM_OK;
+  };
+  if (!on_device && cuda_ok(cudaMalloc(&d_r2c, rbytes), "cudaMalloc(r2c)"))
+    cuda_ok(cudaMemcpyAsync(d_r2c, r2c, rbytes, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(r2c)");
   if (rc == BEAM_OK && !out_on_device)
-    BEAM_CUDA(cudaMemcpyAsync(out, d_out, sizeof(double) * 2 * n2 * n, cudaMemcpyDeviceToHost, s));
-  BEAM_CUDA(cudaStreamSynchronize(s));
+    cuda_ok(cudaMalloc(&d_out, sizeof(double) * 2 * n2 * std::max(1, n)), "cudaMalloc(out)");
+  if (rc == BEAM_OK && cuda_ok(cudaMalloc(&d_jobs, sizeof(int32_t) * 2 * std::max(1, n)), "cudaMalloc(jobs)") &&
+      cuda_ok(cudaMemcpyAsync(d_jobs, planes, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(planes)"))
+    cuda_ok(cudaMemcpyAsync(d_jobs + n, rings, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(rings)");
+  if (rc == BEAM_OK) {
+    size_t before = p->device_bytes;
+    rc = launch_dft<double2>(p, px, on_device ? r2c : d_r2c, d_jobs, d_jobs + n, n,
+                             (double2 *)(out_on_device ? out : d_out), (long long)n2);
+    p->device_bytes = before;
+  }
+  if (rc == BEAM_OK && !out_on_device)
+    cuda_ok(cudaMemcpyAsync(out, d_out, sizeof(double) * 2 * n2 * n, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync(out)");
+  const cudaError_t se = cudaStreamSynchronize(s);  // before the buffers are freed, on every path
+  cuda_ok(se, "cudaStreamSynchronize");
   cudaFree(d_r2c);
   cudaFree(d_out);
   cudaFree(d_jobs);

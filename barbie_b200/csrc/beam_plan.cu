@@ -739,7 +739,12 @@ int count_closed_triangles(beam_gpu_plan *p, std::vector<long long> &counts) {
   build_modes(g, all, ring_first, mode_ij, pixlocal);
   int16_t *d_mode = nullptr;
   BEAM_CUDA(cudaMalloc(&d_mode, sizeof(int16_t) * std::max<size_t>(1, mode_ij.size())));
-  BEAM_CUDA(cudaMemcpy(d_mode, mode_ij.data(), sizeof(int16_t) * mode_ij.size(), cudaMemcpyHostToDevice));
+  const cudaError_t ce = cudaMemcpy(d_mode, mode_ij.data(), sizeof(int16_t) * mode_ij.size(), cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) {
+    cudaFree(d_mode);
+    set_detail(std::string("cudaMemcpy(mode table): ") + cudaGetErrorString(ce));
+    return BEAM_ECUDA;
+  }
   std::vector<int> rps(g.nrp);
   std::iota(rps.begin(), rps.end(), 0);
   std::vector<long long> first;
