@@ -137,7 +137,9 @@ __host__ __device__ constexpr bool fma_pairs_tiles(int ntiles) { return ntiles >
 // Consumer warps of a mixed-path CTA with n tiles, and the most of any class.
 __host__ __device__ constexpr int fma_cons_warps(int n) { return fma_pairs_tiles(n) ? (n + 1) / 2 : n; }
 constexpr int fma_max_cons_warps(int n = 1) {
-  return n > TRI_WARPS ? 0 : (fma_cons_warps(n) > fma_max_cons_warps(n + 1) ? fma_cons_warps(n) : fma_max_cons_warps(n + 1));
+  return n > TRI_WARPS ? 0
+                       : (fma_cons_warps(n) > fma_max_cons_warps(n + 1) ? fma_cons_warps(n)
+                                                                        : fma_max_cons_warps(n + 1));
 }
 
 // Mixed-precision consumer for items of one or two tiles: one tile per warp
