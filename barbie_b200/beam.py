@@ -67,7 +67,7 @@ class PlanInfo(ctypes.Structure):
                 ("n_fourier_terms", ctypes.c_long), ("n_modes", ctypes.c_long), ("n_planes", ctypes.c_int),
                 ("device_bytes", ctypes.c_size_t), ("vol", ctypes.c_double),
                 ("n_shard_terms", ctypes.c_long), ("launches_last_run", ctypes.c_int),
-                ("run_bytes", ctypes.c_size_t)]
+                ("run_bytes", ctypes.c_size_t), ("n_run_combos", ctypes.c_long)]
 
 
 TUNE_MAX, FIELD_TUNE_MAX = 16, 4

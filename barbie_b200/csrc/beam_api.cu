@@ -197,6 +197,7 @@ int beam_gpu_plan_get_info(const beam_gpu_plan *p, beam_plan_info *info) {
   info->vol = p->geom.vol;
   info->launches_last_run = p->main ? p->main->launches : 0;
   info->run_bytes = slot_bytes(p, 1);
+  info->n_run_combos = (long)p->n_run_combos;
   return BEAM_OK;
 }
 

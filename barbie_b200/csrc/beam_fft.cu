@@ -451,30 +451,40 @@ void free_pixel_path(beam_gpu_plan *p) {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[BEAM_NOALLOC_SCRATCH_BYTES];
 alignas(16) static unsigned char g_noalloc_host[BEAM_NOALLOC_SCRATCH_BYTES];
 static std::mutex g_noalloc_mutex;
-constexpr int NOALLOC_MAX_DEVICES = 64;
-static void *g_noalloc_addr[NOALLOC_MAX_DEVICES];  // device address of the scratch array, per device
 
-// Device address of the scratch array on the current device, looked up once
-// per device (with that device current).
-static int noalloc_scratch(int dev, void **ptr) {
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
-    set_detail("device ordinal beyond the allocation-free path's table");
-    return BEAM_EINVAL;
+// Device address of the scratch array in the current device's context, looked
+// up on every call (no allocation; a cached address would go stale after
+// cudaDeviceReset or under another context of the same device).
+static int noalloc_scratch(void **ptr) {
+  void *a = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+  if (e != cudaSuccess || !a) {
+    set_detail(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    return BEAM_ECUDA;
   }
-  if (!g_noalloc_addr[dev]) {
-    void *a = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
-    if (e != cudaSuccess || !a) {
-      set_detail(std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-      return BEAM_ECUDA;
-    }
-    g_noalloc_addr[dev] = a;
-  }
-  *ptr = g_noalloc_addr[dev];
+  *ptr = a;
   return BEAM_OK;
 }
 
 static size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+// Visit the pixels of ring r in row-major order: fn(i, j) for every (i, j)
+// with low <= |k| < high. Only rows and columns with |i|, |j| < high can hold
+// ring pixels, so the scan covers those alone.
+template <typename F>
+static void noalloc_ring_pixels(long NN, double low, double high, const F &fn) {
+  const long lim = std::min(NN / 2, (long)std::ceil(high));  // |i|, |j| <= lim covers |k| < high
+  for (long i = 0; i < NN; ++i) {
+    if (i > lim && i < NN - lim) i = NN - lim;
+    const int ia = (int)((i > NN / 2) ? (i - NN) : i);
+    for (long j = 0; j < NN; ++j) {
+      if (j > lim && j < NN - lim) j = NN - lim;
+      const int ja = (int)((j > NN / 2) ? (j - NN) : j);
+      const double kk = sqrt(1. * (ia * ia + ja * ja));
+      if (kk >= low && kk < high) fn(i, j);
+    }
+  }
+}
 
 }  // namespace beam
 
@@ -500,11 +510,24 @@ extern "C" int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const d
       return BEAM_EINVAL;
     }
   if (n == 0) return BEAM_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The tables travel from a static host buffer that the next call rewrites;
+  // a captured copy would read it at replay time, after that rewrite. So a
+  // capturing stream is refused before any other CUDA call.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BEAM_CUDA(cudaStreamIsCapturing(st, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    set_detail("the allocation-free plane-ring call cannot be captured into a CUDA graph (its tables are staged "
+               "from a host buffer that later calls rewrite)");
+    return BEAM_EINVAL;
+  }
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   int dev = 0;
   BEAM_CUDA(cudaGetDevice(&dev));
+  int smem_optin = 0;
+  BEAM_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   void *scratch = nullptr;
-  BEAM_TRY(noalloc_scratch(dev, &scratch));
+  BEAM_TRY(noalloc_scratch(&scratch));
 
   // ring edges and, for the requested rings, their non-zero rows and modes in
   // row-major order (the order beam_gpu_plane_rings uses)
@@ -517,25 +540,16 @@ extern "C" int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const d
   size_t off_rr = align16(off_jobs + sizeof(int32_t) * 2 * n);
   size_t off_rows = align16(off_rr + sizeof(RingRows) * Nr);
   unsigned char *h = g_noalloc_host;
-  // count rows and modes first, to lay the tables out and check the limit
+  // count rows and modes first, to lay the tables out and check the limits
   long nrows = 0, nmodes = 0;
   int max_rows = 1;
   for (long r = 0; r < Nr; ++r) {
     if (!want[r]) continue;
-    long rows = 0;
-    for (long i = 0; i < NN; ++i) {
-      int ia = (int)((i > NN / 2) ? (i - NN) : i);
-      bool row = false;
-      for (long j = 0; j < NN; ++j) {
-        int ja = (int)((j > NN / 2) ? (j - NN) : j);
-        double kk = sqrt(1. * (ia * ia + ja * ja));
-        if (kk >= low[r] && kk < high[r]) {
-          ++nmodes;
-          row = true;
-        }
-      }
-      rows += row;
-    }
+    long rows = 0, last_i = -1;
+    noalloc_ring_pixels(NN, low[r], high[r], [&](long i, long) {
+      ++nmodes;
+      if (i != last_i) ++rows, last_i = i;
+    });
     nrows += rows;
     max_rows = std::max(max_rows, (int)rows);
   }
@@ -545,6 +559,12 @@ extern "C" int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const d
   if (total > BEAM_NOALLOC_SCRATCH_BYTES) {
     set_detail("the requested rings need " + std::to_string(total) + " bytes of tables; the allocation-free path holds " +
                std::to_string((size_t)BEAM_NOALLOC_SCRATCH_BYTES));
+    return BEAM_EINVAL;
+  }
+  const size_t smem = sizeof(double2) * ((size_t)NN + (size_t)max_rows * PR_YB);
+  if (smem > (size_t)smem_optin) {
+    set_detail("the widest requested ring needs " + std::to_string(smem) + " bytes of shared memory per block; "
+               "the device allows " + std::to_string(smem_optin));
     return BEAM_EINVAL;
   }
   double2 *tw = reinterpret_cast<double2 *>(h + off_tw);
@@ -565,33 +585,36 @@ extern "C" int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const d
   for (long r = 0; r < Nr; ++r) {
     rr[r] = RingRows{(int)at_row, 0};
     if (!want[r]) continue;
-    for (long i = 0; i < NN; ++i) {
-      int ia = (int)((i > NN / 2) ? (i - NN) : i);
-      bool row = false;
-      for (long j = 0; j < NN; ++j) {
-        int ja = (int)((j > NN / 2) ? (j - NN) : j);
-        double kk = sqrt(1. * (ia * ia + ja * ja));
-        if (!(kk >= low[r] && kk < high[r])) continue;
-        if (!row) {
-          row_i[at_row] = (int32_t)i;
-          row_mode[at_row] = (int32_t)at_mode;
-          ++at_row;
-          row = true;
-        }
-        mode_ij[2 * at_mode] = (int16_t)i;
-        mode_ij[2 * at_mode + 1] = (int16_t)j;
-        ++at_mode;
+    long last_i = -1;
+    noalloc_ring_pixels(NN, low[r], high[r], [&](long i, long j) {
+      if (i != last_i) {
+        row_i[at_row] = (int32_t)i;
+        row_mode[at_row] = (int32_t)at_mode;
+        ++at_row;
+        last_i = i;
       }
-    }
+      mode_ij[2 * at_mode] = (int16_t)i;
+      mode_ij[2 * at_mode + 1] = (int16_t)j;
+      ++at_mode;
+    });
     rr[r].n_rows = (int)at_row - rr[r].first_row;
   }
   row_mode[at_row] = (int32_t)at_mode;
 
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The attribute first: a refusal leaves nothing queued. Its error is also
+  // cleared here, so it cannot surface in a later call's launch check.
+  cudaError_t ea = cudaFuncSetAttribute(k_plane_ring_dft<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem);
+  if (ea != cudaSuccess) {
+    (void)cudaGetLastError();
+    set_detail(std::string("cudaFuncSetAttribute(shared memory): ") + cudaGetErrorString(ea));
+    return BEAM_ECUDA;
+  }
   unsigned char *d = static_cast<unsigned char *>(scratch);
+  // From pageable memory the driver stages the tables before this returns
+  // (so the next call may rewrite the host buffer); it may first wait for
+  // the stream's earlier work.
   BEAM_CUDA(cudaMemcpyAsync(d, h, total, cudaMemcpyHostToDevice, st));
-  size_t smem = sizeof(double2) * ((size_t)NN + (size_t)max_rows * PR_YB);
-  BEAM_CUDA(cudaFuncSetAttribute(k_plane_ring_dft<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid((unsigned)((NN + PR_YB - 1) / PR_YB), (unsigned)n);
   k_plane_ring_dft<double2><<<grid, PR_THREADS, smem, st>>>(
       reinterpret_cast<const double2 *>(r2c_dev), (int)NN, reinterpret_cast<const int32_t *>(d + off_jobs),

@@ -74,14 +74,17 @@ void host_parallel(int n, const F &fn) {
 // Device-side status word written by kernels whose waits are bounded.
 enum : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BAD_INDEX = 2 };
 
-// Threads per triangle-sum CTA and in-plane triangles staged per pipeline stage.
-// Triangle-sum decomposition. Each warp owns a tile of TRI_P1 planes p1 x 32
-// planes p3 (one p3 per lane, p2 = -p1-p3) of one ring triplet's accepted
-// (p1, p2) "combos"; a CTA holds up to TRI_WARPS tiles of the same triplet.
-// The triplet's in-plane triangles are listed k2-major, so consecutive
-// triangles sharing k2 form a run; runs are cut into pieces of at most
-// TRI_CHUNK triangles and whole pieces are packed into chunks of at most
-// TRI_CHUNK triangles, one pipeline stage each.
+// Triangle-sum decomposition. Of each ring triplet's three legs, leg 1 (ring
+// r1, plane p1 >= 0) is the "x" leg; of the other two, the plan makes the one
+// whose modes repeat most in the in-plane list the run leg "y" (below: ring
+// r2, plane p2 = -p1-p3) and the other the tile leg "z" (ring r3, plane p3).
+// Each warp owns a tile of TRI_P1 planes p1 x 32 planes p3 (one p3 per lane)
+// of one ring triplet's accepted (p1, p2) "combos"; a CTA holds up to
+// TRI_WARPS tiles of the same triplet. The triplet's in-plane triangles are
+// listed y-major, so consecutive triangles sharing the y mode form a run;
+// runs are packed into chunks of at most TRI_CHUNK triangles and TRI_PIECES
+// pieces (a run's part within one chunk), one pipeline stage each, a run
+// longer than a chunk's room going on in the next chunk.
 constexpr int TRI_WARPS = 7;   // most tiles per CTA (one consumer warp each, plus one producer warp)
 constexpr int TRI_P1 = 8;      // planes p1 per thread
 constexpr int TRI_CHUNK = 16;  // in-plane triangles per stage
@@ -103,11 +106,19 @@ struct TriChunk {
   int pc0;       // first piece in the global piece table
   int packed;    // nt (bits 0-4), npc (bits 5-7), piece lengths (5 bits each from bit 8)
 };
-// fields of TriChunk::packed / TriDesc::packed
+// fields of TriChunk::packed / TriDesc::packed. A run longer than the room
+// left in a chunk continues in the next chunk: the chunk's last piece is then
+// marked CONT_OUT (its outer product is carried, not yet multiplied by the run
+// leg) and the next chunk's first piece CONT_IN (it adds to the carried one).
+constexpr int CHUNK_CONT_IN = 1 << 28, CHUNK_CONT_OUT = 1 << 29;
 __host__ __device__ inline int chunk_nt(int packed) { return packed & 31; }
 __host__ __device__ inline int chunk_npc(int packed) { return (packed >> 5) & 7; }
 __host__ __device__ inline int chunk_len(int packed, int piece) { return (packed >> (8 + 5 * piece)) & 31; }
-__host__ __device__ inline int chunk_pack(int nt, int npc, int lens) { return nt | (npc << 5) | (lens << 8); }
+__host__ __device__ inline bool chunk_cont_in(int packed) { return (packed & CHUNK_CONT_IN) != 0; }
+__host__ __device__ inline bool chunk_cont_out(int packed) { return (packed & CHUNK_CONT_OUT) != 0; }
+__host__ __device__ inline int chunk_pack(int nt, int npc, int lens, int flags = 0) {
+  return nt | (npc << 5) | (lens << 8) | flags;
+}
 
 // What the kernel reads per chunk: the layout and, for each triangle and
 // piece, the row (mode index within its ring) to stage -- one independent
@@ -283,6 +294,7 @@ struct beam_gpu_plan {
   // beam_gpu_plan_autotune
   long long tau0 = beam::TRI_TAU_MAX;
   double balance = 8.0;
+  long long n_run_combos = 0;  // sum over owned triplets of runs x combos (beam_plan_info.n_run_combos)
 };
 
 namespace beam {

@@ -28,6 +28,11 @@ namespace beam {
 // k2 of ring r2 (one thread each), count or list the modes k1 of ring r1 for
 // which k3 = -(k1 + k2) mod NN lies in ring r3. Triangles are emitted k2-major,
 // k1 in ring order, so the list order is deterministic.
+//
+// Which two of the triplet's rings play "r2" and "r3" here is the caller's
+// choice (swap): the run leg ("r2", whose mode a run of the list shares and
+// whose plane is -p1 - p(tile)) and the tile leg ("r3"). The sum is symmetric
+// in the two; the plan takes as run leg the ring whose runs are longer.
 // ---------------------------------------------------------------------------
 struct TripletRef {
   int r1, r2, r3;
@@ -91,7 +96,7 @@ __global__ void k_build_desc(const TriChunk *__restrict__ chunks, long long n, c
 static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, const std::vector<int32_t> &ring_first,
                               const int16_t *d_mode_ij, const int16_t *d_ringmap, const int16_t *d_pixlocal,
                               std::vector<long long> &tri_first, ushort4 **d_list, long long *n_terms,
-                              std::vector<int> *k2cnt) {
+                              std::vector<int> *k2cnt, const std::vector<char> *swap = nullptr) {
   cudaStream_t s = p->ctx->stream;
   const beam_geom &g = p->geom;
   std::vector<TripletRef> refs(rps.size());
@@ -100,9 +105,10 @@ static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, con
   for (size_t u = 0; u < rps.size(); ++u) {
     int rp = rps[u];
     TripletRef &t = refs[u];
+    const bool sw = swap && (*swap)[u];
     t.r1 = g.rp[3 * rp];
-    t.r2 = g.rp[3 * rp + 1];
-    t.r3 = g.rp[3 * rp + 2];
+    t.r2 = g.rp[3 * rp + (sw ? 2 : 1)];
+    t.r3 = g.rp[3 * rp + (sw ? 1 : 2)];
     t.m1 = ring_first[t.r1];
     t.n1 = ring_first[t.r1 + 1] - t.m1;
     t.m2 = ring_first[t.r2];
@@ -225,8 +231,8 @@ static int upload(beam_gpu_plan *p, T **dst, const std::vector<T> &src) {
 // split of partial sums that stay zero, so their triangles come out as B = 0.
 static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, const std::vector<int32_t> &u_ncombo,
                       const std::vector<int32_t> &combo_p1, const std::vector<int32_t> &combo_p2,
-                      const std::vector<int> &k2cnt, const std::vector<char> &own, int A,
-                      std::vector<int32_t> &u_nsplit, std::vector<long long> &u_part) {
+                      const std::vector<int> &k2cnt, const std::vector<char> &own, const std::vector<char> &u_swap,
+                      int A, std::vector<int32_t> &u_nsplit, std::vector<long long> &u_part) {
   const beam_geom &g = p->geom;
   DevPlan &d = p->d;
   auto floorA = [A](int v) { return v - (((v % A) + A) % A); };
@@ -245,8 +251,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   std::vector<std::vector<Group>> groups(d.n_used);
   std::vector<long long> k2base(d.n_used + 1, 0);
   for (int u = 0; u < d.n_used; ++u) {
-    int r2 = g.rp[3 * p->used_rp[u] + 1];
-    k2base[u + 1] = k2base[u] + (p->ring_first[r2 + 1] - p->ring_first[r2]);
+    int ry = g.rp[3 * p->used_rp[u] + (u_swap[u] ? 2 : 1)];  // the run leg's ring
+    k2base[u + 1] = k2base[u] + (p->ring_first[ry + 1] - p->ring_first[ry]);
   }
   // Origin of each triplet's block grid: p1 blocks start at 8 b - o1 (o1 in
   // {0, 4}: the mixed consumer reads a block's planes as aligned float4s),
@@ -374,6 +380,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     for (long long k = k2base[u]; k < k2base[u + 1]; ++k) nruns[u] += (k2cnt[k] > 0);
     for (const Group &gr : groups[u]) wmaxu[u] = std::max(wmaxu[u], (double)gr.ntiles * 256.0 * (double)nt);
   }
+  p->n_run_combos = 0;
+  for (int u = 0; u < d.n_used; ++u) p->n_run_combos += nruns[u] * (long long)u_ncombo[u];
   auto splits = [&](int u, long long tau_max) {
     const long long nt = p->tri_first[u + 1] - p->tri_first[u];
     double want = std::max(std::ceil(wmaxu[u] / target), std::ceil((double)nt / (double)tau_max));
@@ -405,36 +413,49 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     u_nsplit[u] = ns;
     u_part[u + 1] = u_part[u] + (long long)ns * u_ncombo[u];
     int rp = p->used_rp[u];
-    int m1 = p->ring_first[g.rp[3 * rp]], m2 = p->ring_first[g.rp[3 * rp + 1]], m3 = p->ring_first[g.rp[3 * rp + 2]];
+    const int ly = u_swap[u] ? 2 : 1, lz = u_swap[u] ? 1 : 2;  // run leg and tile leg
+    int m1 = p->ring_first[g.rp[3 * rp]], m2 = p->ring_first[g.rp[3 * rp + ly]],
+        m3 = p->ring_first[g.rp[3 * rp + lz]];
     size_t r = 0;
     long long t = p->tri_first[u], done = 0;
     for (int s = 0; s < ns; ++s) {
       long long goal = nt * (s + 1) / ns;
       int ch0 = (int)chunks.size();
-      // chunk under construction: triangles, pieces and piece lengths
+      // chunk under construction: triangles, pieces, piece lengths and the
+      // run-continuation flags
       long long ct0 = t;
-      int cpc0 = (int)pieces.size(), cnt_ = 0, cnpc = 0, clens = 0;
+      int cpc0 = (int)pieces.size(), cnt_ = 0, cnpc = 0, clens = 0, cflags = 0;
       long long tsplit = 0;
       auto close_chunk = [&]() {
-        chunks.push_back(TriChunk{ct0, cpc0, chunk_pack(cnt_, cnpc, clens)});
+        chunks.push_back(TriChunk{ct0, cpc0, chunk_pack(cnt_, cnpc, clens, cflags)});
         tsplit += cnt_;
+        ct0 = t;
+        cpc0 = (int)pieces.size();
+        cnt_ = cnpc = clens = cflags = 0;
       };
       while (r < runs.size() && (done < goal || s == ns - 1)) {
+        // A run that does not fit the chunk's room goes on in the next chunk:
+        // its part here is a whole number of groups of 4 triangles (the FP64
+        // consumer's MMA depth), so only a run's last part can be ragged.
         int left = runs[r].x;
+        bool cont = false;
         while (left > 0) {
-          int len = std::min(left, TRI_CHUNK);
-          if (cnt_ + len > TRI_CHUNK || cnpc == TRI_PIECES) {
-            close_chunk();
-            ct0 = t;
-            cpc0 = (int)pieces.size();
-            cnt_ = cnpc = clens = 0;
-          }
+          if (cnpc == TRI_PIECES || TRI_CHUNK - cnt_ < std::min(left, 4)) close_chunk();
+          const int room = TRI_CHUNK - cnt_;  // >= 4 whenever the run does not fit
+          const int len = left <= room ? left : (room / 4) * 4;
+          const bool more = len < left;
           pieces.push_back(make_int2(len, runs[r].y));
           clens |= len << (5 * cnpc);
+          if (cnpc == 0 && cont) cflags |= CHUNK_CONT_IN;
           cnt_ += len;
           cnpc += 1;
           t += len;
           left -= len;
+          cont = more;
+          if (more) {
+            cflags |= CHUNK_CONT_OUT;
+            close_chunk();
+          }
         }
         done += runs[r].x;
         ++r;
@@ -491,6 +512,17 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     for (char v : seen)
       if (!v) return set_detail("combo without a tile"), BEAM_EINVAL;
     long long covered = 0, piece_sum = 0;
+    for (size_t c = 0; c < chunks.size(); ++c) {
+      const TriChunk &k = chunks[c];
+      if (chunk_cont_out(k.packed)) {
+        // the next chunk carries the run on: same run mode, no piece after it here
+        if (c + 1 >= chunks.size() || !chunk_cont_in(chunks[c + 1].packed) ||
+            pieces[chunks[c + 1].pc0].y != pieces[k.pc0 + chunk_npc(k.packed) - 1].y)
+          return set_detail("run continuation"), BEAM_EINVAL;
+      }
+      if (chunk_cont_in(k.packed) && (c == 0 || !chunk_cont_out(chunks[c - 1].packed)))
+        return set_detail("run continuation"), BEAM_EINVAL;
+    }
     for (const TriChunk &k : chunks) {
       int nt = chunk_nt(k.packed), npc = chunk_npc(k.packed), lsum = 0;
       covered += nt;
@@ -651,10 +683,41 @@ int build_plan_tables(beam_gpu_plan *p) {
   std::vector<int32_t> combo_out(ntri);
   for (long long c = 0; c < ntri; ++c) combo_out[c] = p->bin_pos[combo_tid[c]];
 
-  // in-plane triangle lists (GPU), k2-major: k2cnt holds each run's length
+  // Run leg of each used triplet: of rings r2 and r3, the one with fewer
+  // distinct modes in the triplet's in-plane list, so its runs are longer and
+  // the product with the run leg (once per run and accepted triangle) is paid
+  // fewer times. At NN=384 this lengthens the mean run (weighted by work) from
+  // 17 to 50 triangles. Both orientations are counted on the GPU.
+  std::vector<char> u_swap(d.n_used, 0);
+  {
+    std::vector<char> all(d.n_used, 1);
+    std::vector<long long> f2, f3;
+    std::vector<int> c2, c3;
+    BEAM_TRY(enumerate_in_plane(p, p->used_rp, p->ring_first, d.mode_ij, d.ringmap, nullptr, f2, nullptr, nullptr,
+                                &c2, nullptr));
+    BEAM_TRY(enumerate_in_plane(p, p->used_rp, p->ring_first, d.mode_ij, d.ringmap, nullptr, f3, nullptr, nullptr,
+                                &c3, &all));
+    size_t a2 = 0, a3 = 0;
+    for (int u = 0; u < d.n_used; ++u) {
+      const int rp = p->used_rp[u], r2 = g.rp[3 * rp + 1], r3 = g.rp[3 * rp + 2];
+      const int n2 = p->ring_first[r2 + 1] - p->ring_first[r2], n3 = p->ring_first[r3 + 1] - p->ring_first[r3];
+      long long runs2 = 0, runs3 = 0;
+      for (int k = 0; k < n2; ++k) runs2 += (c2[a2 + k] > 0);
+      for (int k = 0; k < n3; ++k) runs3 += (c3[a3 + k] > 0);
+      u_swap[u] = runs3 < runs2;
+      a2 += n2;
+      a3 += n3;
+    }
+  }
+  // the tile axis of a triplet is the tile leg's plane; combo_p2 below holds
+  // the run leg's plane (p3 for a swapped triplet), the tile's p3 = -p1 - it
+  for (long long c = 0; c < ntri; ++c)
+    if (u_swap[combo_u[c]]) combo_p2[c] = -combo_p1[c] - combo_p2[c];
+
+  // in-plane triangle lists (GPU), run-leg-major: k2cnt holds each run's length
   std::vector<int> k2cnt;
   BEAM_TRY(enumerate_in_plane(p, p->used_rp, p->ring_first, d.mode_ij, d.ringmap, d.pixlocal, p->tri_first,
-                              &d.tri_list, &d.n_terms, &k2cnt));
+                              &d.tri_list, &d.n_terms, &k2cnt, &u_swap));
 
   // epilogue tables in bin order
   std::vector<double> ep_px(ntri), ep_pz(ntri), ep_ana(ntri);
@@ -683,7 +746,7 @@ int build_plan_tables(beam_gpu_plan *p) {
   // work decomposition of the triangle-sum kernel
   std::vector<int32_t> u_nsplit;
   std::vector<long long> u_part;
-  BEAM_TRY(build_work(p, u_cfirst, u_ncombo, combo_p1, combo_p2, k2cnt, own, A, u_nsplit, u_part));
+  BEAM_TRY(build_work(p, u_cfirst, u_ncombo, combo_p1, combo_p2, k2cnt, own, u_swap, A, u_nsplit, u_part));
   d.n_part = u_part[d.n_used];
   u_part.pop_back();
   u_cfirst.pop_back();

@@ -165,6 +165,7 @@ __device__ __forceinline__ void tri_consume_fma_tile(const TriArgs &a, const Tri
   const int oz = any ? p3 + a.colbase - it.colz : 0;                  // z read
   const int oy0 = any ? -p1b - p3 + a.colbase - it.coly : TRI_P1 - 1;  // y reads oy0 - q
   double sum[TRI_P1];
+  unsigned long long wr[TRI_P1 / 2] = {}, wi[TRI_P1 / 2] = {};  // the run's W, planes (2h, 2h+1), across chunks
 #pragma unroll
   for (int q = 0; q < TRI_P1; ++q) sum[q] = 0.0;
   int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
@@ -180,9 +181,10 @@ __device__ __forceinline__ void tri_consume_fma_tile(const TriArgs &a, const Tri
     int tt = 0;
     for (int pc = 0; pc < npc; ++pc) {
       const int len = chunk_len(packed, pc);
-      unsigned long long wr[TRI_P1 / 2], wi[TRI_P1 / 2];  // planes (2h, 2h+1)
+      if (pc != 0 || !chunk_cont_in(packed)) {
 #pragma unroll
-      for (int h = 0; h < TRI_P1 / 2; ++h) wr[h] = wi[h] = 0ull;
+        for (int h = 0; h < TRI_P1 / 2; ++h) wr[h] = wi[h] = 0ull;
+      }
       for (int j = 0; j < len; ++j, ++tt) {
         const float *zr = zs + 2 * tt * it.Lz + mixed_re(oz);
         const float z_re = zr[0], z_im = zr[4];
@@ -204,6 +206,7 @@ __device__ __forceinline__ void tri_consume_fma_tile(const TriArgs &a, const Tri
           fma2(wi[g / 2 + 1], r1, ZI);
         }
       }
+      if (pc == npc - 1 && chunk_cont_out(packed)) break;  // the run goes on in the next chunk
       const float *yr = ys + 2 * pc * it.Ly;
 #pragma unroll
       for (int h = 0; h < TRI_P1 / 2; ++h) {
@@ -268,6 +271,7 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
   // and coly are), and a lane without combos reads columns 2..8
   const int oy0 = any ? -P1 - P3 + a.colbase - it.coly : 8;
   double sum[4][4];
+  unsigned long long wr[4][2] = {}, wi[4][2] = {};  // the run's W, [c][planes (2h, 2h+1)], across chunks
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -285,9 +289,10 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
     int tt = 0;
     for (int pc = 0; pc < npc; ++pc) {
       const int len = chunk_len(packed, pc);
-      unsigned long long wr[4][2], wi[4][2];  // [c][planes (2h, 2h+1)]
+      if (pc != 0 || !chunk_cont_in(packed)) {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) wr[c][0] = wr[c][1] = wi[c][0] = wi[c][1] = 0ull;
+        for (int c = 0; c < 4; ++c) wr[c][0] = wr[c][1] = wi[c][0] = wi[c][1] = 0ull;
+      }
       for (int k = 0; k < len; ++k, ++tt) {
         const float *xr = xs + 2 * tt * it.Lx + 2 * ox;  // block ox / 4: 4 real, then 4 imaginary parts
         const float *zr = zs + 2 * tt * it.Lz + 2 * oz;
@@ -319,6 +324,7 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
           }
         }
       }
+      if (pc == npc - 1 && chunk_cont_out(packed)) break;  // the run goes on in the next chunk
       // y of the 7 planes p2 the patch spans, (i, c) reading y[i + c] =
       // column oy0 - i - c: column oy0 is the first of its 4-column block,
       // oy0 - 4 .. oy0 - 1 the whole block before it, oy0 - 6 and oy0 - 5
@@ -372,20 +378,23 @@ __device__ __forceinline__ void dmma884(double &d0, double &d1, double av, doubl
 }
 
 // The pieces of one staged chunk for a tile with NB blocks in use: per group
-// of four triangles, x and z loads and four MMAs per block; at each piece's
-// end, sum += Re(y W) per combo. Blocks NB..3 of a tile hold no combos and
-// are skipped.
+// of four triangles, x and z loads and four MMAs per block; at each run's
+// end, sum += Re(y W) per combo. A run that goes on in the next chunk keeps
+// its W (carried in wr/wi) and is multiplied by y there. Blocks NB..3 of a
+// tile hold no combos and are skipped.
 template <int NB>
 __device__ __forceinline__ void dmma_pieces(const double2 *xs, const double2 *zs, const double2 *ys, int px, int pz,
                                             int Ly, int packed, const int (&ox)[4], const int (&oz)[4],
-                                            const int (&oyb)[4], int t, double (&sum)[4][2]) {
+                                            const int (&oyb)[4], int t, double (&wr)[4][2], double (&wi)[4][2],
+                                            double (&sum)[4][2]) {
   const int npc = chunk_npc(packed);
   int tt = 0;
   for (int pc = 0; pc < npc; ++pc) {
     const int len = chunk_len(packed, pc);
-    double wr[NB][2], wi[NB][2];
+    if (pc != 0 || !chunk_cont_in(packed)) {
 #pragma unroll
-    for (int n = 0; n < NB; ++n) wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
+      for (int n = 0; n < NB; ++n) wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
+    }
     // one group of four triangles; only a piece's last group can be partial
     // (CHECK: its rows past the piece's end are zeroed)
     auto group = [&](int k0, auto check) {
@@ -416,6 +425,7 @@ __device__ __forceinline__ void dmma_pieces(const double2 *xs, const double2 *zs
     for (; k0 + 4 <= len; k0 += 4) group(k0, std::false_type{});
     if (k0 < len) group(k0, std::true_type{});
     tt += len;
+    if (pc == npc - 1 && chunk_cont_out(packed)) break;  // the run goes on in the next chunk
     const double2 *yr = ys + pc * Ly;
 #pragma unroll
     for (int n = 0; n < NB; ++n)
@@ -459,9 +469,9 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
     oz[n] = (unsigned)o < (unsigned)it.Lz ? o : 0;
     oyb[n] = -(tl.p1_0[n] + g) - (tl.p3_0[n] + 2 * t) + a.colbase - it.coly;  // y of (n, e): oyb[n] - e
   }
-  double sum[4][2];
+  double sum[4][2], wr[4][2], wi[4][2];  // wr/wi: the current run's W, carried across chunks
 #pragma unroll
-  for (int n = 0; n < 4; ++n) sum[n][0] = sum[n][1] = 0.0;
+  for (int n = 0; n < 4; ++n) sum[n][0] = sum[n][1] = wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
   int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
   for (int c = 0; c < nch; ++c) {
     const int s = c % TRI_STAGES;
@@ -472,10 +482,10 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
     const double2 *zs = xs + TRI_CHUNK * px;
     const double2 *ys = zs + TRI_CHUNK * pz;
     switch (nblk) {  // warp-uniform: the tile's blocks in use
-      case 1: dmma_pieces<1>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
-      case 2: dmma_pieces<2>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
-      case 3: dmma_pieces<3>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
-      default: dmma_pieces<4>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, sum); break;
+      case 1: dmma_pieces<1>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, wr, wi, sum); break;
+      case 2: dmma_pieces<2>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, wr, wi, sum); break;
+      case 3: dmma_pieces<3>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, wr, wi, sum); break;
+      default: dmma_pieces<4>(xs, zs, ys, px, pz, it.Ly, packed, ox, oz, oyb, t, wr, wi, sum); break;
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(smem_addr(&empty[s]));

@@ -60,7 +60,7 @@ def parse_args():
     ap.add_argument("--no-field", action="store_true", help="skip the field generation / ingestion timing")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default work decomposition and FFT tiles (no beam_gpu_*_autotune)")
-    ap.add_argument("--serve-jobs", type=int, default=40, help="jobs per precision in the serving stream")
+    ap.add_argument("--serve-jobs", type=int, default=200, help="jobs per precision in the serving stream")
     ap.add_argument("--batch-pool", type=int, default=64, help="distinct fields cycled over the batch")
     return ap.parse_args()
 
@@ -150,6 +150,40 @@ def measured_fp64_peak(torch, device) -> float:
     return 2.0 * n ** 3 / (best / 1e3) / 1e12
 
 
+def measured_fp32_peak(torch, device) -> float:
+    """cuBLAS SGEMM throughput (TFLOP/s) with TF32 off, i.e. FP32 FMA on the
+    CUDA cores: best of 5 at 8192^3."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(n, n, dtype=torch.float32, device=device)
+        b = torch.randn(n, n, dtype=torch.float32, device=device)
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        torch.cuda.empty_cache()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
+def triangle_flops(info) -> float:
+    """Algorithmic flops of one bispectrum's triangle sums: a complex
+    multiply-accumulate per closed in-plane triangle term (x_k1 z_k3 into the
+    run's outer product: 8 flop), and per (run, accepted triangle) the product
+    with the run's third leg, Re(y W), added to the triangle's sum (4 flop)."""
+    return 8.0 * info["n_fourier_terms"] + 4.0 * info["n_run_combos"]
+
+
 def profile_traffic(kernel: str):
     """DRAM bytes per launch of a kernel from a committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_nn384.md")
@@ -177,6 +211,24 @@ def mixed_errors(fp64: dict, mixed: dict) -> dict:
             "counts_identical": bool(np.array_equal(fp64["count"], mixed["count"]))}
 
 
+def oracle_fixture_bins(field):
+    """Bins of the committed oracle fixture of the benchmark workload
+    (tests/golden/oracle_nn384_cfg3.npz: the oracle's pixel sums on the
+    benchmark's first field), shaped as a run's result, or None when the
+    fixture is absent or belongs to another field."""
+    import hashlib
+    path = os.path.join(ROOT, "tests", "golden", "oracle_nn384_cfg3.npz")
+    if not os.path.exists(path):
+        return None
+    g = np.load(path)
+    if str(g["field_sha256"]) != hashlib.sha256(field.tobytes()).hexdigest():
+        return None
+    vol = float(WORKLOAD["NN"]) ** 3
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out = g["bs"] / (vol * g["norm"])
+    return {"out": out, "norm": g["norm"], "count": g["counts"]}
+
+
 # --------------------------------------------------------------------- ours
 def run_ours(args):
     import torch
@@ -193,8 +245,20 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     W = WORKLOAD
     ctx = beam.Context(local)
+    fields = [synth_field(W["NN"], realization_seed(1 + rank * args.fields + i)) for i in range(args.fields)]
+    dev_fields = [torch.from_numpy(f).to(dev) for f in fields]
+    host_fields = [torch.from_numpy(f).pin_memory() for f in fields]
+    host_np = [h.numpy() for h in host_fields]
+    torch.cuda.synchronize(dev)
+    # cold start: plan creation (geometry, triangle lists, work decomposition;
+    # no autotuning) and the first bispectrum from a pinned host field, host clock
+    t0 = time.perf_counter()
     plan = beam.Plan(ctx, W["NN"], W["UL_k1"], W["LL_k1"], W["BW_k1"], Nmax=W["Nmax"], Nr=W["Nr"],
                      n_mtbin=W["n_mtbin"])
+    t1 = time.perf_counter()
+    plan.run(host_np[0])
+    t2 = time.perf_counter()
+    cold = {"plan_create_ms": (t1 - t0) * 1e3, "first_run_ms": (t2 - t1) * 1e3, "total_ms": (t2 - t0) * 1e3}
     tuning = {"fp64": tune_plan(plan, args)}
     info = plan.info
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -211,10 +275,6 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    fields = [synth_field(W["NN"], realization_seed(1 + rank * args.fields + i)) for i in range(args.fields)]
-    dev_fields = [torch.from_numpy(f).to(dev) for f in fields]
-    host_fields = [torch.from_numpy(f).pin_memory() for f in fields]
-    host_np = [h.numpy() for h in host_fields]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
 
     def timed_loop(p, srcs, steps):
@@ -274,19 +334,38 @@ def run_ours(args):
         mixed = {"value": world * args.steps / (m_total / 1e3) * 3600.0, "unit": UNIT,
                  "ms_per_step": m_total / args.steps, "triangle_kernel_ms": float(np.mean(mtri)),
                  "speedup_vs_fp64": (sum(times) / sum(mt)), **mixed_errors(ref, got)}
+        oracle_ref = oracle_fixture_bins(fields[0]) if rank == 0 else None
+        if oracle_ref is not None:
+            mixed["vs_oracle"] = {k: v for k, v in mixed_errors(oracle_ref, got).items()
+                                  if k in ("max_rel_err", "median_rel_err", "frac_within_1e-5")}
         plan_m.close()
+    else:
+        oracle_ref = oracle_fixture_bins(fields[0]) if rank == 0 else None
+
+    # FP64 bins against the oracle's bins of the same field (committed fixture)
+    fp64_vs_oracle = None
+    if oracle_ref is not None:
+        e = mixed_errors(oracle_ref, plan.run(dev_fields[0]))
+        fp64_vs_oracle = {"max_rel_err": e["max_rel_err"], "median_rel_err": e["median_rel_err"],
+                          "bins_compared": e["bins_compared"], "counts_identical": e["counts_identical"]}
 
     # roofline of the dominant kernel (triangle sums on the FP64 tensor pipe, mma.sync m8n8k4.f64)
     peak = measured_fp64_peak(torch, dev)
     tri_avg = float(np.mean(tri_ms))
-    flops = 10.0 * info["n_fourier_terms"]  # complex a*b (6) + Re(ab*c) (3) + accumulate (1)
+    flops = triangle_flops(info)
     achieved = flops / (tri_avg / 1e3) / 1e12
     roofline = {"kernel": "k_triangle<double2>", "bound": "tensor", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": profile_traffic("k_triangle"),
                 "flops_per_launch": flops, "launch_ms": tri_avg,
+                "flop_basis": "8 per closed in-plane triangle term + 4 per (run, accepted triangle)",
                 "peak_source": ("FP64 tensor pipe: cuBLAS DGEMM 8192^3 measured in this run "
-                                "(MEASURED_PEAKS.json has no FP64 figure)"),
-                "pixel_equivalent_tflops": 4.0 * info["n_triples"] * W["NN"] ** 2 / (tri_avg / 1e3) / 1e12}
+                                "(MEASURED_PEAKS.json has no FP64 figure)")}
+    if mixed is not None:
+        p32 = measured_fp32_peak(torch, dev)
+        a32 = flops / (mixed["triangle_kernel_ms"] / 1e3) / 1e12
+        mixed["roofline"] = {"kernel": "k_triangle<float2>", "bound": "fp32", "achieved": a32, "peak": p32,
+                             "unit": "TFLOP/s", "frac": a32 / p32,
+                             "peak_source": "FP32 FMA: cuBLAS SGEMM 8192^3, TF32 off, measured in this run"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -299,6 +378,8 @@ def run_ours(args):
     # build, one triangle-sum launch per tile class, split reduction, epilogue
     per_run = plan.refresh_info()["launches_last_run"]
     gpu_launches = per_run * args.steps
+    # The printed line keeps the headline numbers as top-level scalars and stays
+    # short; every section in full goes to stderr as one "bench details:" line.
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -306,15 +387,35 @@ def run_ours(args):
         "config": {"workload": WORKLOAD_NAME, **W, "path": "plain FP64, closed in-plane triangle sums",
                    "parallelism": f"replicas x{world} (one realization per rank per step)",
                    "l2": "flushed between steps (256 MiB write, outside the timed events)",
-                   "n_triples": info["n_triples"], "n_fourier_terms": info["n_fourier_terms"],
-                   "plan_device_bytes": info["device_bytes"]},
+                   "serve_jobs": args.serve_jobs if serving else 0},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_total / args.steps},
-        "latency": lat, "wall_s": wall, "clocks": clk, "roofline": roofline, "mixed": mixed,
-        "cpu_baseline": cpu, "gpu_launches": gpu_launches, "batched": batched, "serving": serving,
-        "field": field, "autotune": tuning,
+        "clocks": clk, "gpu_launches": gpu_launches,
+        "roofline": {k: roofline[k] for k in ("kernel", "bound", "achieved", "peak", "unit", "frac", "traffic")},
+        "cpu_baseline": ({k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")} if cpu else None),
+        "fp64_max_rel_err_vs_oracle": fp64_vs_oracle["max_rel_err"] if fp64_vs_oracle else None,
+        "mixed_value": mixed["value"] if mixed else None,
+        "mixed_speedup": mixed["speedup_vs_fp64"] if mixed else None,
+        "mixed_max_rel_err": mixed["max_rel_err"] if mixed else None,
+        "mixed_median_rel_err": mixed["median_rel_err"] if mixed else None,
+        "mixed_roofline_frac": mixed["roofline"]["frac"] if mixed else None,
+        "serve_jobs": args.serve_jobs if serving else 0,
+        "serve_p50_ms": serving["fp64"]["p50_ms"] if serving else None,
+        "serve_p99_ms": serving["fp64"]["p99_ms"] if serving else None,
+        "serve_mixed_p50_ms": serving["mixed"]["p50_ms"] if serving else None,
+        "serve_mixed_p99_ms": serving["mixed"]["p99_ms"] if serving else None,
+        "batched_value": batched["mixed"]["batch_of_16"]["value"] if batched else None,
+        "batched_fp64_value": batched["fp64"]["batch_of_16"]["value"] if batched else None,
+        "cold_start_ms": cold["total_ms"],
+        "latency_p50_ms": lat["p50_ms"], "latency_p99_ms": lat["p99_ms"],
     }
+    details = {"roofline": roofline, "mixed": mixed, "fp64_vs_oracle": fp64_vs_oracle, "cpu_baseline": cpu,
+               "cold_start": cold, "latency": lat, "wall_s": wall, "batched": batched, "serving": serving,
+               "field": field, "autotune": tuning,
+               "plan": {"n_triples": info["n_triples"], "n_fourier_terms": info["n_fourier_terms"],
+                        "n_run_combos": info["n_run_combos"], "plan_device_bytes": info["device_bytes"]}}
     if rank == 0:
+        print("bench details: " + json.dumps(details), file=sys.stderr, flush=True)
         print(json.dumps(line), flush=True)
     plan.close()
     ctx.close()

@@ -125,6 +125,9 @@ typedef struct beam_plan_info {
   long n_shard_terms;     /* in-plane triangles this plan's shard sums (n_fourier_terms unsharded) */
   int launches_last_run;  /* kernels the plan's last beam_gpu_run / triangle_sums call launched */
   size_t run_bytes;       /* device bytes of the buffers of one more concurrent realization */
+  long n_run_combos;      /* sum over accepted triangles of the runs of their triplet's in-plane list
+                             (triangles sharing the mode of the leg whose plane is -p1 - p(tile), whose
+                             product with the run's accumulated outer product is formed once per run) */
 } beam_plan_info;
 
 /* Library / device setup. Replaces the fftw_init_threads / plan_with_nthreads
@@ -193,15 +196,19 @@ BEAM_API int beam_gpu_plane_rings(beam_gpu_plan *plan, const double *r2c, int r2
  * planes/rings are host arrays of n entries (0 <= plane < Nmax <= NN/2,
  * 0 <= ring < Nr, Nr a multiple of 10). Work is queued on `stream` (a
  * cudaStream_t, NULL for the legacy default stream) of the current device and
- * the call returns without waiting for it.
+ * the call returns without waiting for the transform. The tables are staged
+ * from pageable host memory, so the call may first wait for the work already
+ * queued on `stream`.
  * The ring tables, twiddles and job list go to a fixed scratch array of
  * BEAM_NOALLOC_SCRATCH_BYTES in the library's device image; each GPU that
  * loads the library holds that array until the process exits. A call whose
- * tables need more (many rings or large NN), or n > BEAM_NOALLOC_MAX_JOBS,
- * returns BEAM_EINVAL and explains in beam_gpu_last_error_detail(). The first
- * call on a device looks the array's address up once (make that first call
- * before any stream capture). Every call rewrites the array, so calls whose
- * work overlaps on the GPU race on it: order them on one stream. */
+ * tables need more (many rings or large NN), whose widest ring needs more
+ * shared memory than the device allows, or with n > BEAM_NOALLOC_MAX_JOBS,
+ * returns BEAM_EINVAL before queuing anything and explains in
+ * beam_gpu_last_error_detail(). The call cannot be captured into a CUDA graph:
+ * given a capturing stream it returns BEAM_EINVAL. Every call rewrites the
+ * array, so calls whose work overlaps on the GPU race on it: order them on one
+ * stream. */
 #define BEAM_NOALLOC_SCRATCH_BYTES (2u * 1024u * 1024u)
 #define BEAM_NOALLOC_MAX_JOBS 4096
 BEAM_API int beam_gpu_plane_rings_noalloc(long NN, long Nmax, long Nr, const double *r2c_dev, const int *planes,

@@ -85,6 +85,13 @@ int orc_estimate(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1, i
                  double LL, const double *r2c, double *bin_bs, double *bin_norm, double *bin_out,
                  int64_t *counts, double *tri_B, long tri_cap, int nthreads, double *bin_ana);
 
+/* orc_estimate with the per-triangle pixel sums accumulated in long double
+ * when wide != 0 (same pixel order; the bins then carry far less of the
+ * oracle's own rounding, for fixtures at NN >= 384). */
+int orc_estimate_ex(long NN, long Nmax, long Nr, int UL_k1, int LL_k1, int BW_k1, int n_mtbin,
+                    double LL, const double *r2c, double *bin_bs, double *bin_norm, double *bin_out,
+                    int64_t *counts, double *tri_B, long tri_cap, int nthreads, double *bin_ana, int wide);
+
 /* barbie.c:300-305: analytic redshift-space bispectrum of a triangle from its
  * sorted legs (|K_i|, p_i) in grid units, cell size LL: P(k) = k^-2
  * (input_ps, funcs.c:73-81), ff = 0.1, beta = 1 (barbie.c:79-80). */

@@ -75,6 +75,8 @@ def lib() -> ctypes.CDLL:
                                    ctypes.c_int, ctypes.c_int, ctypes.c_double, dp, dp, dp, dp,
                                    ctypes.POINTER(ctypes.c_int64), dp, ctypes.c_long, ctypes.c_int, dp]
         L.orc_estimate.restype = ctypes.c_int
+        L.orc_estimate_ex.argtypes = L.orc_estimate.argtypes + [ctypes.c_int]
+        L.orc_estimate_ex.restype = ctypes.c_int
         L.orc_biana.argtypes = [ctypes.c_long, ctypes.c_double, dp, dp]
         L.orc_biana.restype = ctypes.c_double
         L.orc_biana_all.argtypes = [ctypes.c_long, ctypes.c_double, ctypes.c_void_p, ctypes.c_long, dp]
@@ -235,8 +237,9 @@ def biana(tri: np.ndarray, NN: int, LL: float = 1.0) -> np.ndarray:
 
 
 def estimate(r2c: np.ndarray, NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin=5, LL=1.0,
-             nthreads=None, want_B=False):
+             nthreads=None, want_B=False, wide=False):
     """The full estimator (barbie.c:110-397) with the plane-ring cache in RAM.
+    wide: accumulate each triangle's pixel sum in long double (orc_estimate_ex).
 
     Returns dict(bs, norm, out, counts, ana, ana_out[, B]) with bins shaped
     [n_k1bin][n_mtbin][n_mtbin][16] (counts without the pole axis)."""
@@ -250,10 +253,10 @@ def estimate(r2c: np.ndarray, NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin=5, LL=1
         ntri = len(enumerate_triples(NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin)[0])
         B = np.zeros(max(ntri, 1))
     nthreads = nthreads or os.cpu_count() or 1
-    rc = lib().orc_estimate(NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin, LL,
-                            _dp(np.ascontiguousarray(r2c, dtype=np.float64)), _dp(bs), _dp(nm), _dp(out),
-                            counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
-                            _dp(B) if B is not None else None, ntri, nthreads, _dp(ana))
+    rc = lib().orc_estimate_ex(NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, n_mtbin, LL,
+                               _dp(np.ascontiguousarray(r2c, dtype=np.float64)), _dp(bs), _dp(nm), _dp(out),
+                               counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                               _dp(B) if B is not None else None, ntri, nthreads, _dp(ana), int(bool(wide)))
     if rc != 0:
         raise RuntimeError(f"orc_estimate failed ({rc})")
     with np.errstate(divide="ignore", invalid="ignore"):

@@ -25,9 +25,25 @@ oracle/_ref/field_ref against the FFTW shim and the GSL stand-in, whose normal
 deviates are the Philox stream of oracle/philox_normal.h): r2c
 float64[NN][NN][NN+2] and the printed sigma.
 
-Usage: python tests/golden/make_golden.py [--pk | --field] [case ...]   (default:
-all cases; --pk makes only the pk_<case>.npz files, --field only the field ones)
-Needs the reference sources (to build oracle/_ref) -- run where they exist.
+oracle_<case>.npz holds the raw bin sums of cases at the benchmark's and the
+serving form's sizes, where the reference program would need its 9-21 GB disk
+cache and hours of its single-threaded loop: the oracle's restatement
+(oracle/beam_oracle.c, orc_estimate_ex, pixel sums over the plane-ring
+transforms as barbie.c:315-337 in pixel order, each accumulated in long double
+so that the oracle's own rounding stays far below the 1e-10 bar where bins
+cancel by ~1e5, threaded over triangles) -- pinned to the reference program
+on the cases above -- gives
+  bs, norm, ana  float64[n_k1bin][n_mtbin][n_mtbin][16]: bin_BS_real,
+                 bin_normalization and the analytic sum before barbie.c:390
+  counts         int64[n_k1bin][n_mtbin][n_mtbin]: closed triangles with B != 0
+  field_sha256, the configuration and the oracle's wall time.
+
+Usage: python tests/golden/make_golden.py [--pk | --field | --oracle] [case ...]
+(default: all reference cases; --pk makes only the pk_<case>.npz files, --field
+only the field ones, --oracle the oracle_<case>.npz ones). Needs the reference
+sources (to build oracle/_ref) -- run where they exist; --oracle needs only the
+oracle library, RAM for the plane-ring arrays (9.4 GB at NN=384, 21 GB at
+NN=512) and takes minutes per case on 8 cores.
 """
 from __future__ import annotations
 
@@ -64,6 +80,16 @@ CASES = {
     "nn96_r20": (96, 32, 20, 21, 1, 1, 3),
     # the drop-in comparison case: NN=256, Nmax=64, Nr=30, bins 1..31 width 1
     "nn256_cfg2": (256, 64, 30, 31, 1, 1, 1),
+}
+
+# name: (NN, Nmax, Nr, UL_k1, LL_k1, BW_k1, realization) of the oracle fixtures
+ORACLE_CASES = {
+    # the benchmark workload `barbie 384 1 51 1 1` on the benchmark's first field
+    "nn384_cfg3": (384, 100, 40, 51, 1, 1, 1),
+    # served shapes: NN=192 with 30 rings to 60 and k1 bins of width 2 over
+    # 1..61; NN=512 with 40 rings to 128, k1 bins 1..31 (of 1..129)
+    "nn192_serve": (192, 60, 30, 61, 1, 2, 4),
+    "nn512_serve": (512, 128, 40, 31, 1, 1, 5),
 }
 
 
@@ -128,14 +154,41 @@ def run_field_case(name: str, scratch: str) -> str:
     return out
 
 
+def run_oracle_case(name: str, save_B: str | None = None) -> str:
+    from oracle import oracle_py
+    NN, Nmax, Nr, UL, LL, BW, r = ORACLE_CASES[name]
+    field = synth_field(NN, realization_seed(r))
+    t = time.time()
+    res = oracle_py.estimate(field, NN, Nmax, Nr, UL, LL, BW, want_B=save_B is not None, wide=True)
+    secs = time.time() - t
+    out = os.path.join(HERE, f"oracle_{name}.npz")
+    np.savez_compressed(out, bs=res["bs"], norm=res["norm"], ana=res["ana"], counts=res["counts"],
+                        field_sha256=hashlib.sha256(field.tobytes()).hexdigest(),
+                        config=np.array([NN, Nmax, Nr, UL, LL, BW, r], dtype=np.int64), seconds=secs)
+    if save_B:  # per-triangle sums in loop order (large; not a committed fixture)
+        np.save(save_B, res["B"])
+    print(f"oracle_{name}: {int((res['norm'][..., 0] > 0.1).sum())} printed bins in {secs:.1f} s -> {out}")
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("cases", nargs="*", default=list(CASES))
+    ap.add_argument("cases", nargs="*")
     ap.add_argument("--pk", action="store_true", help="only the power-spectrum multipole fixtures")
     ap.add_argument("--field", action="store_true", help="only the field generator fixtures")
+    ap.add_argument("--oracle", action="store_true", help="the oracle fixtures of large cases")
+    ap.add_argument("--save-B", default=None, help="with --oracle and one case: .npy path for its per-triangle B")
     ap.add_argument("--scratch", default=os.path.join(HERE, ".scratch"))
     args = ap.parse_args()
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
+    if args.oracle:
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
+        for c in args.cases or list(ORACLE_CASES):
+            run_oracle_case(c, args.save_B)
+        return
+    args.cases = args.cases or list(CASES)
+    sys.path.insert(0, ROOT)
+    from __graft_entry__ import reference_dir
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", f"REF={reference_dir()}"], check=True)
     if not os.path.exists(REF_BIN):
         sys.exit("oracle/_ref/barbie_ref is missing: the reference sources are needed to build it")
     if args.field:
