@@ -67,7 +67,7 @@ class PlanInfo(ctypes.Structure):
                 ("n_fourier_terms", ctypes.c_long), ("n_modes", ctypes.c_long), ("n_planes", ctypes.c_int),
                 ("device_bytes", ctypes.c_size_t), ("vol", ctypes.c_double),
                 ("n_shard_terms", ctypes.c_long), ("launches_last_run", ctypes.c_int),
-                ("run_bytes", ctypes.c_size_t), ("n_run_combos", ctypes.c_long)]
+                ("run_bytes", ctypes.c_size_t), ("n_run_combos", ctypes.c_long), ("build_ms", ctypes.c_float * 5)]
 
 
 TUNE_MAX, FIELD_TUNE_MAX = 16, 4
@@ -116,6 +116,7 @@ def load() -> ctypes.CDLL:
     L.beam_gpu_plan_create.argtypes = [vp, ctypes.POINTER(Cfg), ctypes.POINTER(vp)]
     L.beam_gpu_plan_destroy.argtypes = [vp]
     L.beam_gpu_plan_destroy.restype = None
+    L.beam_gpu_plan_set_triangle_launch.argtypes = [vp, ctypes.c_int]
     L.beam_gpu_plan_get_info.argtypes = [vp, ctypes.POINTER(PlanInfo)]
     L.beam_gpu_run.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Result)]
     L.beam_gpu_run_batch.argtypes = [vp, ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(Result)]
@@ -233,7 +234,7 @@ class Plan:
         ctx._plans.add(self)
         info = PlanInfo()
         _check(L.beam_gpu_plan_get_info(h, ctypes.byref(info)), "beam_gpu_plan_get_info")
-        self.info = {k: getattr(info, k) for k, _ in PlanInfo._fields_}
+        self.info = {k: (list(getattr(info, k)) if k == "build_ms" else getattr(info, k)) for k, _ in PlanInfo._fields_}
         self.n_k1bin = info.n_k1bin
         self.shape = (info.n_k1bin, n_mtbin, n_mtbin, NPOLES)
         self.NN = NN
@@ -277,11 +278,16 @@ class Plan:
         _check(_lib.beam_gpu_run_batch_ex(self._h, addrs, len(fields), results, batch), "beam_gpu_run_batch_ex")
         return out
 
+    def set_triangle_launch(self, mode: str) -> None:
+        """'classes' (one launch per tile class, the default) or 'persistent' (one launch for all)."""
+        m = {"classes": 0, "persistent": 1}[mode]
+        _check(_lib.beam_gpu_plan_set_triangle_launch(self._h, m), "beam_gpu_plan_set_triangle_launch")
+
     def refresh_info(self) -> dict:
         """Re-read beam_gpu_plan_get_info (device bytes and launch count change as the plan runs)."""
         info = PlanInfo()
         _check(_lib.beam_gpu_plan_get_info(self._h, ctypes.byref(info)), "beam_gpu_plan_get_info")
-        self.info = {k: getattr(info, k) for k, _ in PlanInfo._fields_}
+        self.info = {k: (list(getattr(info, k)) if k == "build_ms" else getattr(info, k)) for k, _ in PlanInfo._fields_}
         return self.info
 
     def triangle_sums(self, r2c) -> np.ndarray:

@@ -1,4 +1,5 @@
 // C-ABI entry points of libbeam_gpu (declared in include/beam_gpu.h).
+#include <chrono>
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -110,6 +111,7 @@ void beam_gpu_destroy(beam_gpu_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->field_ws) cudaFree(ctx->field_ws);
   if (ctx->scratch) cudaFree(ctx->scratch);
+  if (ctx->pk_tab) cudaFree(ctx->pk_tab);
   lane_destroy(&ctx->lane);
   delete ctx;
 }
@@ -133,12 +135,20 @@ int beam_gpu_plan_create(beam_gpu_ctx *ctx, const beam_cfg *cfg, beam_gpu_plan *
   p->ctx = ctx;
   p->cfg = *cfg;
   p->cfg.shard_count = shards;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+    return (float)std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  const auto t0 = now();
   int rc = beam_geom_build(&p->geom, cfg);
+  p->build_ms[0] = ms(t0, now());
   if (rc == BEAM_EBOUNDS) set_detail("a triangle's (k1, t, mu) bin falls outside the bin arrays");
   if (rc == BEAM_EINVAL) set_detail("invalid configuration (NN even, Nmax <= NN/2, Nr a multiple of 10, "
                                     "BW_k1 > 0 dividing UL_k1 - LL_k1 > 0)");
   if (rc == BEAM_OK) rc = host_guard([&] { return build_plan_tables(p); });
+  const auto t1 = now();
   if (rc == BEAM_OK) rc = host_guard([&] { return slot_create(p, 1, &ctx->lane, &p->main); });
+  p->build_ms[4] = ms(t1, now());
   if (rc == BEAM_OK && pixel_method(p)) rc = host_guard([&] { return build_pixel_path(p); });
   if (rc != BEAM_OK) {
     beam_gpu_plan_destroy(p);
@@ -162,6 +172,22 @@ void beam_gpu_plan_destroy(beam_gpu_plan *p) {
   free_plan_tables(p);
   beam_geom_free(&p->geom);
   delete p;
+}
+
+int beam_gpu_plan_set_triangle_launch(beam_gpu_plan *p, int mode) {
+  if (!p || (mode != BEAM_LAUNCH_CLASSES && mode != BEAM_LAUNCH_PERSISTENT)) return BEAM_EINVAL;
+  if (p->tri_launch == mode) return BEAM_OK;
+  BEAM_CUDA(cudaSetDevice(p->ctx->device));
+  BEAM_CUDA(cudaStreamSynchronize(p->ctx->stream));
+  for (RunSlot *s : {p->main, p->batch[0], p->batch[1]}) {
+    if (!s || !s->graph) continue;
+    if (s->done) BEAM_CUDA(cudaEventSynchronize(s->done));
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    s->graph_n = 0;
+  }
+  p->tri_launch = mode;
+  return BEAM_OK;
 }
 
 int beam_gpu_plan_get_info(const beam_gpu_plan *p, beam_plan_info *info) {
@@ -198,6 +224,7 @@ int beam_gpu_plan_get_info(const beam_gpu_plan *p, beam_plan_info *info) {
   info->launches_last_run = p->main ? p->main->launches : 0;
   info->run_bytes = slot_bytes(p, 1);
   info->n_run_combos = (long)p->n_run_combos;
+  for (int k = 0; k < 5; ++k) info->build_ms[k] = p->build_ms[k];
   return BEAM_OK;
 }
 

@@ -190,6 +190,7 @@ struct DevPlan {
   TriDesc *descs = nullptr;       // [n_chunks], read by the kernel
   int n_items = 0;
   TriItem *items = nullptr;       // [n_items]: grouped by tile count, largest work first in a group
+  int32_t *q_order = nullptr;     // [n_items] items in decreasing order of work (persistent kernel)
   int class_first[TRI_WARPS + 2] = {};  // items with n tiles: [class_first[n], class_first[n+1])
   int class_stage[TRI_WARPS + 1] = {};  // stage size (complex values) of the CTAs with n tiles
   long long n_part = 0;           // partial-sum slots per realization
@@ -235,7 +236,7 @@ struct RunSlot {
   double *bins = nullptr;         // [cap][BIN_SECTIONS][n_bins][16]: bs, norm, out, analytic sum
   long long *bin_count = nullptr; // [cap][n_bins]
   double *ep_part = nullptr;      // [cap][n_epchunks][33] epilogue chunk sums
-  int *status = nullptr;          // device status word
+  int *status = nullptr;          // device status word, then the persistent triangle kernel's work counter
   double *h_staging = nullptr;    // pinned [cap][n_modes][Q]
   double *h_bins = nullptr;       // pinned [cap][BIN_SECTIONS][n_bins][16]
   long long *h_count = nullptr;   // pinned [cap][n_bins]
@@ -269,6 +270,14 @@ struct beam_gpu_ctx {
   // small per-context scratch (power-multipole partial sums), kept between calls
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
+  // power multipoles: the geometry of the last (NN, Nbin) -- per visited mode
+  // class its Legendre weights and bin (beam_pk.cu) and the per-bin sums that
+  // do not depend on the field -- kept for the next call with the same sizes
+  void *pk_tab = nullptr;
+  size_t pk_tab_bytes = 0;
+  long pk_NN = 0;
+  int pk_Nbin = 0;
+  std::vector<double> pk_geo;
 };
 
 struct beam_gpu_plan {
@@ -295,6 +304,8 @@ struct beam_gpu_plan {
   long long tau0 = beam::TRI_TAU_MAX;
   double balance = 8.0;
   long long n_run_combos = 0;  // sum over owned triplets of runs x combos (beam_plan_info.n_run_combos)
+  float build_ms[5] = {};      // creation phases (beam_plan_info.build_ms)
+  int tri_launch = BEAM_LAUNCH_CLASSES;  // how the triangle sums are launched (BEAM_LAUNCH_*)
 };
 
 namespace beam {

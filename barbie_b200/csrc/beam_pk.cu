@@ -169,36 +169,73 @@ __device__ __forceinline__ int pk_bin(float m, const float *t, int Nbin) {
   return lo;
 }
 
+// Geometry of the visited modes for the table-driven row kernel: entry
+// [key(lo, hi)][c] of the modes (a, b, c) with {a, b} = {lo, hi} (lo <= hi <=
+// NN/2; key = hi (hi + 1) / 2 + lo) holds P2, P4, P6 and the bin (as int bits,
+// -1 outside the bins), computed with the row kernel's own expressions
+// (fac a a + fac b b is the same float either way round).
+__host__ __device__ inline long pk_key(long lo, long hi) { return hi * (hi + 1) / 2 + lo; }
+
+__global__ void k_pk_table(int NN, int Nbin, float fac, PkEdges edges, float4 *__restrict__ tab) {
+  const long N = NN, NH = N / 2 + 1, hi = blockIdx.y;
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (hi + 1) * NH) return;
+  const long lo = e / NH, c = e - lo * NH, a = lo, b = hi;
+  const float ab = fac * a * a + fac * b * b;
+  const float m = __fsqrt_rn(ab + fac * c * c);
+  int d = pk_bin(m, edges.t, Nbin);
+  float P2 = 0.f, P4 = 0.f, P6 = 0.f;
+  if (d >= 0) {
+    const float mu = __fdiv_rn((float)c, N * m);
+    P2 = (float)(0.5 * (3. * mu * mu - 1.));
+    const double m2 = (double)mu * mu;
+    const float mu4 = (float)(m2 * m2), mu6 = (float)(m2 * m2 * m2);
+    P4 = (float)(0.125 * (35.0 * mu4 - 30.0 * mu * mu + 3));
+    P6 = (float)(0.0625 * (231.0 * mu6 - 315.0 * mu4 + 105.0 * mu * mu - 5));
+  } else {
+    d = -1;
+  }
+  tab[pk_key(lo, hi) * NH + c] = make_float4(P2, P4, P6, __int_as_float(d));
+}
+
+// NV = 9: every sum of a bin from the modes themselves. NV = 4 with TAB: the
+// field-dependent sums alone (|Delta|^2 and its P2, P4, P6 copies), the
+// Legendre weights and bins read from the geometry table; each sum is formed
+// in the same order either way, so both give the same bits.
 // 3 CTAs per SM, as many as shared memory allows: at most 85 registers per thread
-// (98 unbounded, 2 CTAs per SM; 0.46 -> 0.38 ms at NN=384, bit-identical)
-__global__ void __launch_bounds__(PK_THREADS, 3) k_pk_rows(const double2 *__restrict__ r2c, int NN, int Nbin, float fac,
-                                                        PkEdges edges, double *__restrict__ part) {
-  __shared__ double acc[PK_THREADS / 32][PK_FAST_BINS * PK_VALS];
+// (98 unbounded, 2 CTAs per SM; 0.46 -> 0.38 ms at NN=384, bit-identical); the
+// table-driven form keeps fewer values and fits 4 CTAs per SM
+template <int NV, bool TAB>
+__global__ void __launch_bounds__(PK_THREADS, TAB ? 4 : 3) k_pk_rows(const double2 *__restrict__ r2c, int NN, int Nbin, float fac,
+                                                        PkEdges edges, const float4 *__restrict__ tab,
+                                                        double *__restrict__ part) {
+  __shared__ double acc[PK_THREADS / 32][PK_FAST_BINS * NV];
   __shared__ float te[PK_FAST_BINS + 1];
   __shared__ double2 zbuf[PK_THREADS / 32][32 * PK_ROW_LOADS];
+  __shared__ float4 tbuf[PK_THREADS / 32][TAB ? 32 * PK_ROW_LOADS : 1];  // the table rows of the same modes
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long N = NN, NH = N / 2 + 1, half = N / 2;
   for (int q = threadIdx.x; q <= Nbin; q += PK_THREADS) te[q] = edges.t[q];
-  for (int q = lane; q < Nbin * PK_VALS; q += 32) acc[warp][q] = 0.0;
+  for (int q = lane; q < Nbin * NV; q += 32) acc[warp][q] = 0.0;
   __syncthreads();
   // per-lane running sums of the warp's current bin D (warp-uniform), added
   // to the warp's accumulators by a fixed shuffle tree when the bin changes
-  double r[PK_VALS];
+  double r[NV];
 #pragma unroll
-  for (int t = 0; t < PK_VALS; ++t) r[t] = 0.0;
+  for (int t = 0; t < NV; ++t) r[t] = 0.0;
   int D = -1;
   auto flush = [&]() {
     if (D >= 0) {
 #pragma unroll
-      for (int t = 0; t < PK_VALS; ++t) {
+      for (int t = 0; t < NV; ++t) {
         double s = r[t];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) acc[warp][D * PK_VALS + t] += s;
+        if (lane == 0) acc[warp][D * NV + t] += s;
       }
     }
 #pragma unroll
-    for (int t = 0; t < PK_VALS; ++t) r[t] = 0.0;
+    for (int t = 0; t < NV; ++t) r[t] = 0.0;
   };
   for (int rr = 0; rr < PK_ROWS / (PK_THREADS / 32); ++rr) {
     const long row = (long)blockIdx.x * PK_ROWS + warp + (PK_THREADS / 32) * rr;
@@ -207,18 +244,24 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_pk_rows(const double2 *__rest
     // every mode a row contributes has a = fold(i), b = fold(j) (funcs.c:925-1048)
     const long a = (i > half) ? N - i : i, b = (j > half) ? N - j : j;
     const float ab = fac * a * a + fac * b * b;
+    const float4 *trow = TAB ? tab + pk_key(a < b ? a : b, a < b ? b : a) * NH : nullptr;
     const double2 *rowp = r2c + row * NH;
     for (long g0 = 0; g0 < NH; g0 += 32 * PK_ROW_LOADS) {
       // the group's loads first, all in flight at once, into the warp's buffer
       {
         double2 zg[PK_ROW_LOADS];
+        float4 tg[TAB ? PK_ROW_LOADS : 1];
 #pragma unroll
         for (int q = 0; q < PK_ROW_LOADS; ++q) {
           const long c = g0 + 32 * q + lane;
           zg[q] = c < NH ? rowp[c] : make_double2(0.0, 0.0);
+          if (TAB) tg[TAB ? q : 0] = c < NH ? __ldg(trow + c) : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
         }
 #pragma unroll
-        for (int q = 0; q < PK_ROW_LOADS; ++q) zbuf[warp][32 * q + lane] = zg[q];
+        for (int q = 0; q < PK_ROW_LOADS; ++q) {
+          zbuf[warp][32 * q + lane] = zg[q];
+          if (TAB) tbuf[warp][TAB ? 32 * q + lane : 0] = tg[TAB ? q : 0];
+        }
         __syncwarp();
       }
 #pragma unroll 1
@@ -227,11 +270,21 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_pk_rows(const double2 *__rest
       if (k0 >= NH) break;
       const long c = k0 + lane;
       int d = -1;
-      double v[PK_VALS];
+      double v[NV];
 #pragma unroll
-      for (int t = 0; t < PK_VALS; ++t) v[t] = 0.0;
+      for (int t = 0; t < NV; ++t) v[t] = 0.0;
       long bb;
-      if (c < NH && pk_visit(i, j, c, N, &bb) >= 0) {
+      if (TAB) {
+        if (c < NH && pk_visit(i, j, c, N, &bb) >= 0) {
+          const float4 g = tbuf[warp][TAB ? 32 * q + lane : 0];
+          d = __float_as_int(g.w);
+          if (d >= 0) {
+            const double2 z = zbuf[warp][32 * q + lane];
+            const double pw = (z.x * z.x) + (z.y * z.y);
+            v[0] = pw, v[1] = pw * g.x, v[2] = pw * g.y, v[3] = pw * g.z;
+          }
+        }
+      } else if (c < NH && pk_visit(i, j, c, N, &bb) >= 0) {
         const float m = __fsqrt_rn(ab + fac * c * c);  // = (float)sqrt((double)...), see pk_mode
         d = pk_bin(m, te, Nbin);
         if (d >= 0) {
@@ -243,8 +296,11 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_pk_rows(const double2 *__rest
           const float P4 = (float)(0.125 * (35.0 * mu4 - 30.0 * mu * mu + 3));
           const float P6 = (float)(0.0625 * (231.0 * mu6 - 315.0 * mu4 + 105.0 * mu * mu - 5));
           const double pw = (z.x * z.x) + (z.y * z.y);
-          v[0] = pw, v[1] = pw * P2, v[2] = pw * P4, v[3] = pw * P6, v[4] = (double)m, v[5] = 1.0;
-          v[6] = (double)(P2 * P2), v[7] = (double)(P4 * P4), v[8] = (double)(P6 * P6);
+          v[0] = pw, v[1] = pw * P2, v[2] = pw * P4, v[3] = pw * P6;
+          if (NV > 4) {
+            v[4 % NV] = (double)m, v[5 % NV] = 1.0;
+            v[6 % NV] = (double)(P2 * P2), v[7 % NV] = (double)(P4 * P4), v[8 % NV] = (double)(P6 * P6);
+          }
         }
       }
       const int dmax = __reduce_max_sync(0xffffffffu, d);
@@ -252,7 +308,7 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_pk_rows(const double2 *__rest
       const int dmin = (int)__reduce_min_sync(0xffffffffu, d >= 0 ? (unsigned)d : 0xffffffffu);
       if (dmin == dmax && dmax == D) {
 #pragma unroll
-        for (int t = 0; t < PK_VALS; ++t) r[t] += v[t];
+        for (int t = 0; t < NV; ++t) r[t] += v[t];
         continue;
       }
       flush();
@@ -261,13 +317,13 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_pk_rows(const double2 *__rest
         // counted bins of a row are non-decreasing in k), run tails add
         const int ds = d < dmax ? d : -1;
 #pragma unroll
-        for (int t = 0; t < PK_VALS; ++t) r[t] = ds >= 0 ? v[t] : 0.0;
+        for (int t = 0; t < NV; ++t) r[t] = ds >= 0 ? v[t] : 0.0;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
           const int db = __shfl_up_sync(0xffffffffu, ds, off);
           const bool same = lane >= off && db == ds;
 #pragma unroll
-          for (int t = 0; t < PK_VALS; ++t) {
+          for (int t = 0; t < NV; ++t) {
             const double y = __shfl_up_sync(0xffffffffu, r[t], off);
             if (same) r[t] += y;
           }
@@ -275,33 +331,33 @@ __global__ void __launch_bounds__(PK_THREADS, 3) k_pk_rows(const double2 *__rest
         const int dn = __shfl_down_sync(0xffffffffu, ds, 1);
         if (ds >= 0 && (lane == 31 || dn != ds))
 #pragma unroll
-          for (int t = 0; t < PK_VALS; ++t) acc[warp][ds * PK_VALS + t] += r[t];
+          for (int t = 0; t < NV; ++t) acc[warp][ds * NV + t] += r[t];
         __syncwarp();
       }
       D = dmax;
 #pragma unroll
-      for (int t = 0; t < PK_VALS; ++t) r[t] = d == dmax ? v[t] : 0.0;
+      for (int t = 0; t < NV; ++t) r[t] = d == dmax ? v[t] : 0.0;
       }
       __syncwarp();
     }
   }
   flush();
   __syncthreads();
-  for (int q = threadIdx.x; q < Nbin * PK_VALS; q += PK_THREADS) {
+  for (int q = threadIdx.x; q < Nbin * NV; q += PK_THREADS) {
     double s = 0.0;
     for (int w = 0; w < PK_THREADS / 32; ++w) s += acc[w][q];
-    part[(size_t)blockIdx.x * Nbin * PK_VALS + q] = s;
+    part[(size_t)blockIdx.x * Nbin * NV + q] = s;
   }
 }
 
 // Sum of nblk partials in a fixed order: one CTA per value, strided thread
 // sums, then a fixed shuffle / shared-memory tree.
-__global__ void __launch_bounds__(256) k_pk_total(const double *__restrict__ part, int nblk, int Nbin,
+__global__ void __launch_bounds__(256) k_pk_total(const double *__restrict__ part, int nblk, int Nbin, int nv,
                                                   double *__restrict__ tot) {
   __shared__ double w8[8];
   const int q = blockIdx.x;
   double s = 0.0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[(size_t)b * Nbin * PK_VALS + q];
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[(size_t)b * Nbin * nv + q];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) w8[threadIdx.x >> 5] = s;
@@ -386,20 +442,70 @@ extern "C" int beam_gpu_power_multipoles(beam_gpu_ctx *ctx, long NN, double LL, 
   // the reference's float constants (funcs.c:898-900,922)
   const float fac = 1. / (1. * NN * NN);
   const float scale = log10(0.5 * NN) / Nbin;
+  std::vector<double> q((size_t)Nbin * PK_VALS);
+  cudaError_t e = cudaSuccess;
   if (fast) {
     PkEdges edges;
     pk_edges(NN, Nbin, scale, &edges);
-    k_pk_rows<<<(unsigned)nblk, PK_THREADS, 0, st>>>((const double2 *)src, (int)NN, Nbin, fac, edges, part);
+    // The bins' geometric sums (mean |k|, mode count, sums of P_l^2) and each
+    // mode's weights and bin depend on NN and Nbin alone: the first call with
+    // these sizes forms every sum from the modes and keeps the geometry (a
+    // table of at most PK_TAB_MAX bytes); later calls read the table and form
+    // only the field's sums, in the same order.
+    constexpr size_t PK_TAB_MAX = 256ull << 20;
+    const long NH = NN / 2 + 1;
+    const size_t tab_bytes = sizeof(float4) * (size_t)pk_key(0, NH) * (size_t)NH;
+    const bool cached = ctx->pk_tab && ctx->pk_NN == NN && ctx->pk_Nbin == Nbin;
+    if (cached) {
+      k_pk_rows<4, true><<<(unsigned)nblk, PK_THREADS, 0, st>>>((const double2 *)src, (int)NN, Nbin, fac, edges,
+                                                                 (const float4 *)ctx->pk_tab, part);
+      k_pk_total<<<(unsigned)(Nbin * 4), 256, 0, st>>>(part, (int)nblk, Nbin, 4, tot);
+      std::vector<double> f((size_t)Nbin * 4);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(f.data(), tot, sizeof(double) * f.size(), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      for (int d = 0; d < Nbin; ++d)
+        for (int t = 0; t < PK_VALS; ++t)
+          q[(size_t)d * PK_VALS + t] = t < 4 ? f[(size_t)d * 4 + t] : ctx->pk_geo[(size_t)d * PK_VALS + t];
+    } else {
+      k_pk_rows<PK_VALS, false><<<(unsigned)nblk, PK_THREADS, 0, st>>>((const double2 *)src, (int)NN, Nbin, fac, edges,
+                                                                       nullptr, part);
+      k_pk_total<<<(unsigned)(Nbin * PK_VALS), 256, 0, st>>>(part, (int)nblk, Nbin, PK_VALS, tot);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(q.data(), tot, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      // keep the geometry for the next call, when the table fits its bound
+      if (e == cudaSuccess && tab_bytes <= PK_TAB_MAX) {
+        if (ctx->pk_tab_bytes < tab_bytes) {
+          if (ctx->pk_tab) cudaFree(ctx->pk_tab);
+          ctx->pk_tab = nullptr;
+          ctx->pk_tab_bytes = 0;
+          if (cudaMalloc(&ctx->pk_tab, tab_bytes) == cudaSuccess)
+            ctx->pk_tab_bytes = tab_bytes;
+          else
+            (void)cudaGetLastError();  // no table: later calls form every sum, as this one
+        }
+        ctx->pk_NN = 0;
+        if (ctx->pk_tab) {
+          dim3 grid((unsigned)((NH * NH + 255) / 256), (unsigned)NH);
+          k_pk_table<<<grid, 256, 0, st>>>((int)NN, Nbin, fac, edges, (float4 *)ctx->pk_tab);
+          if (cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(st) == cudaSuccess) {
+            ctx->pk_NN = NN;
+            ctx->pk_Nbin = Nbin;
+            ctx->pk_geo = q;
+          }
+        }
+      }
+    }
   } else {
     const size_t smem = sizeof(double) * (size_t)Nbin * PK_VALS;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_pk_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_pk_planes<<<(unsigned)NN, PK_THREADS, smem, st>>>((const double2 *)src, (int)NN, Nbin, fac, scale, part);
+    k_pk_total<<<(unsigned)(Nbin * PK_VALS), 256, 0, st>>>(part, (int)nblk, Nbin, PK_VALS, tot);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(q.data(), tot, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   }
-  k_pk_total<<<(unsigned)(Nbin * PK_VALS), 256, 0, st>>>(part, (int)nblk, Nbin, tot);
-  std::vector<double> q((size_t)Nbin * PK_VALS);
-  cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(q.data(), tot, sizeof(double) * q.size(), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   release();
   if (e != cudaSuccess) {
     set_detail(std::string("power multipoles: ") + cudaGetErrorString(e));

@@ -15,6 +15,7 @@
 // (funcs.c:396-399 computes NN^2 times their number), so they depend only on
 // the geometry and are listed once per plan.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <numeric>
 #include <thread>
@@ -38,7 +39,38 @@ struct TripletRef {
   int r1, r2, r3;
   int m1, n1, m2, n2, m3;  // first mode and mode count of rings r1, r2; first mode of r3
   long long k2base;        // first per-k2 counter of this triplet
+  long long k3base;        // first per-k3 counter (k_tri_count_both)
 };
+
+// (NN - u - v) mod NN for u, v in [0, NN), without a division
+__device__ __forceinline__ int neg_sum_mod(int u, int v, int NN) {
+  int w = NN - u - v;
+  w += (w < 0) ? NN : 0;
+  return w >= NN ? w - NN : w;
+}
+
+// Counts in both orientations at once: per mode k2 of ring r2 the triangles
+// sharing it (one thread each, as k_tri_count), and per mode k3 of ring r3 the
+// triangles sharing that, by atomic increments (integer counts: the order does
+// not matter).
+__global__ void k_tri_count_both(const TripletRef *trip, const int16_t *__restrict__ mode_ij,
+                                 const int16_t *__restrict__ ringmap, const int16_t *__restrict__ pixlocal, int NN,
+                                 int *__restrict__ cnt2, int *__restrict__ cnt3) {
+  const TripletRef t = trip[blockIdx.y];
+  int k2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k2 >= t.n2) return;
+  int i2 = mode_ij[2 * (t.m2 + k2)], j2 = mode_ij[2 * (t.m2 + k2) + 1];
+  int n = 0;
+  for (int k1 = 0; k1 < t.n1; ++k1) {
+    int i1 = mode_ij[2 * (t.m1 + k1)], j1 = mode_ij[2 * (t.m1 + k1) + 1];
+    const int pix = neg_sum_mod(i1, i2, NN) * NN + neg_sum_mod(j1, j2, NN);
+    if (ringmap[pix] == t.r3) {
+      ++n;
+      atomicAdd(&cnt3[t.k3base + pixlocal[pix]], 1);
+    }
+  }
+  cnt2[t.k2base + k2] = n;
+}
 
 __global__ void k_tri_count(const TripletRef *trip, const int16_t *__restrict__ mode_ij,
                             const int16_t *__restrict__ ringmap, int NN, int *__restrict__ cnt) {
@@ -49,8 +81,7 @@ __global__ void k_tri_count(const TripletRef *trip, const int16_t *__restrict__ 
   int n = 0;
   for (int k1 = 0; k1 < t.n1; ++k1) {
     int i1 = mode_ij[2 * (t.m1 + k1)], j1 = mode_ij[2 * (t.m1 + k1) + 1];
-    int i3 = (2 * NN - i1 - i2) % NN, j3 = (2 * NN - j1 - j2) % NN;
-    n += (ringmap[i3 * NN + j3] == t.r3);
+    n += (ringmap[neg_sum_mod(i1, i2, NN) * NN + neg_sum_mod(j1, j2, NN)] == t.r3);
   }
   cnt[t.k2base + k2] = n;
 }
@@ -65,9 +96,9 @@ __global__ void k_tri_write(const TripletRef *trip, const int16_t *__restrict__ 
   long long at = offs[t.k2base + k2];
   for (int k1 = 0; k1 < t.n1; ++k1) {
     int i1 = mode_ij[2 * (t.m1 + k1)], j1 = mode_ij[2 * (t.m1 + k1) + 1];
-    int i3 = (2 * NN - i1 - i2) % NN, j3 = (2 * NN - j1 - j2) % NN;
-    if (ringmap[i3 * NN + j3] == t.r3)
-      out[at++] = make_ushort4((unsigned short)k1, (unsigned short)k2, (unsigned short)pixlocal[i3 * NN + j3], 0);
+    const int pix = neg_sum_mod(i1, i2, NN) * NN + neg_sum_mod(j1, j2, NN);
+    if (ringmap[pix] == t.r3)
+      out[at++] = make_ushort4((unsigned short)k1, (unsigned short)k2, (unsigned short)pixlocal[pix], 0);
   }
 }
 
@@ -96,7 +127,8 @@ __global__ void k_build_desc(const TriChunk *__restrict__ chunks, long long n, c
 static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, const std::vector<int32_t> &ring_first,
                               const int16_t *d_mode_ij, const int16_t *d_ringmap, const int16_t *d_pixlocal,
                               std::vector<long long> &tri_first, ushort4 **d_list, long long *n_terms,
-                              std::vector<int> *k2cnt, const std::vector<char> *swap = nullptr) {
+                              std::vector<int> *k2cnt, const std::vector<char> *swap = nullptr,
+                              const std::vector<int> *given = nullptr) {
   cudaStream_t s = p->ctx->stream;
   const beam_geom &g = p->geom;
   std::vector<TripletRef> refs(rps.size());
@@ -136,8 +168,17 @@ static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, con
     }
     return rc == BEAM_OK;
   };
-  if (cuda_ok(cudaMalloc(&d_refs, sizeof(TripletRef) * refs.size()), "cudaMalloc(triplets)") &&
-      cuda_ok(cudaMalloc(&d_cnt, sizeof(int) * k2total), "cudaMalloc(counts)") &&
+  if (given) {  // counts from an earlier pass in the same orientation
+    if ((long long)given->size() != k2total) {
+      set_detail("in-plane triangle counts of another orientation");
+      return BEAM_EINVAL;
+    }
+    cnt = *given;
+  }
+  if (cuda_ok(cudaMalloc(&d_refs, sizeof(TripletRef) * refs.size()), "cudaMalloc(triplets)") && given) {
+    cuda_ok(cudaMemcpyAsync(d_refs, refs.data(), sizeof(TripletRef) * refs.size(), cudaMemcpyHostToDevice, s),
+            "cudaMemcpyAsync(triplets)");
+  } else if (rc == BEAM_OK && cuda_ok(cudaMalloc(&d_cnt, sizeof(int) * k2total), "cudaMalloc(counts)") &&
       cuda_ok(cudaMemcpyAsync(d_refs, refs.data(), sizeof(TripletRef) * refs.size(), cudaMemcpyHostToDevice, s),
               "cudaMemcpyAsync(triplets)")) {
     for (size_t y0 = 0; y0 < refs.size(); y0 += 65535) {
@@ -178,6 +219,96 @@ static int enumerate_in_plane(beam_gpu_plan *p, const std::vector<int> &rps, con
   cudaFree(d_cnt);
   cudaFree(d_offs);
   return rc;
+}
+
+// In-plane triangle counts of the used triplets in both orientations (run leg
+// r2 or r3): c2 per mode of r2 and c3 per mode of r3, triplet after triplet.
+static int count_both_orientations(beam_gpu_plan *p, const int16_t *d_mode_ij, const int16_t *d_ringmap,
+                                   const int16_t *d_pixlocal, std::vector<int> &c2, std::vector<int> &c3) {
+  cudaStream_t s = p->ctx->stream;
+  const beam_geom &g = p->geom;
+  const std::vector<int> &rps = p->used_rp;
+  std::vector<TripletRef> refs(rps.size());
+  long long tot2 = 0, tot3 = 0;
+  int max_n2 = 1;
+  for (size_t u = 0; u < rps.size(); ++u) {
+    const int rp = rps[u];
+    TripletRef &t = refs[u];
+    t.r1 = g.rp[3 * rp];
+    t.r2 = g.rp[3 * rp + 1];
+    t.r3 = g.rp[3 * rp + 2];
+    t.m1 = p->ring_first[t.r1];
+    t.n1 = p->ring_first[t.r1 + 1] - t.m1;
+    t.m2 = p->ring_first[t.r2];
+    t.n2 = p->ring_first[t.r2 + 1] - t.m2;
+    t.m3 = p->ring_first[t.r3];
+    t.k2base = tot2;
+    t.k3base = tot3;
+    tot2 += t.n2;
+    tot3 += p->ring_first[t.r3 + 1] - t.m3;
+    max_n2 = std::max(max_n2, t.n2);
+  }
+  c2.assign(tot2, 0);
+  c3.assign(tot3, 0);
+  if (rps.empty()) return BEAM_OK;
+  TripletRef *d_refs = nullptr;
+  int *d2 = nullptr, *d3 = nullptr;
+  int rc = BEAM_OK;
+  auto cuda_ok = [&](cudaError_t e, const char *what) {
+    if (rc == BEAM_OK && e != cudaSuccess) {
+      set_detail(std::string(what) + ": " + cudaGetErrorString(e));
+      rc = BEAM_ECUDA;
+    }
+    return rc == BEAM_OK;
+  };
+  if (cuda_ok(cudaMalloc(&d_refs, sizeof(TripletRef) * refs.size()), "cudaMalloc(triplets)") &&
+      cuda_ok(cudaMalloc(&d2, sizeof(int) * std::max<long long>(1, tot2)), "cudaMalloc(counts)") &&
+      cuda_ok(cudaMalloc(&d3, sizeof(int) * std::max<long long>(1, tot3)), "cudaMalloc(counts)") &&
+      cuda_ok(cudaMemsetAsync(d3, 0, sizeof(int) * std::max<long long>(1, tot3), s), "cudaMemsetAsync(counts)") &&
+      cuda_ok(cudaMemcpyAsync(d_refs, refs.data(), sizeof(TripletRef) * refs.size(), cudaMemcpyHostToDevice, s),
+              "cudaMemcpyAsync(triplets)")) {
+    for (size_t y0 = 0; y0 < refs.size(); y0 += 65535) {
+      dim3 grid((max_n2 + 127) / 128, (unsigned)std::min<size_t>(65535, refs.size() - y0));
+      k_tri_count_both<<<grid, 128, 0, s>>>(d_refs + y0, d_mode_ij, d_ringmap, d_pixlocal, (int)g.NN, d2, d3);
+    }
+    if (cuda_ok(cudaGetLastError(), "k_tri_count_both") &&
+        cuda_ok(cudaMemcpyAsync(c2.data(), d2, sizeof(int) * tot2, cudaMemcpyDeviceToHost, s), "counts") &&
+        cuda_ok(cudaMemcpyAsync(c3.data(), d3, sizeof(int) * tot3, cudaMemcpyDeviceToHost, s), "counts"))
+      cuda_ok(cudaStreamSynchronize(s), "k_tri_count_both");
+  }
+  cudaFree(d_refs);
+  cudaFree(d2);
+  cudaFree(d3);
+  return rc;
+}
+
+// Stable counting sort of n items by key(t) in [0, nb), on up to 16 host
+// threads: pos[t] is item t's place in key order (ties in index order), first
+// (nb + 1 entries) each key's first place. Each thread counts its own range of
+// items; a key's places go to the ranges in order, so the result is the one
+// pass in index order gives.
+template <typename K>
+static void stable_bucket_sort(long long n, int nb, const K &key, std::vector<int32_t> &pos,
+                               std::vector<int32_t> &first) {
+  const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::vector<int32_t>> cnt(nt, std::vector<int32_t>(nb, 0));
+  host_parallel(nt, [&](int k) {
+    for (long long t = n * k / nt; t < n * (k + 1) / nt; ++t) cnt[k][key(t)]++;
+  });
+  first.assign(nb + 1, 0);
+  for (int b = 0; b < nb; ++b) {
+    int32_t at = first[b];
+    for (int k = 0; k < nt; ++k) {
+      const int32_t c = cnt[k][b];
+      cnt[k][b] = at;  // thread k's first place in key b
+      at += c;
+    }
+    first[b + 1] = at;
+  }
+  pos.assign(n, 0);
+  host_parallel(nt, [&](int k) {
+    for (long long t = n * k / nt; t < n * (k + 1) / nt; ++t) pos[t] = cnt[k][key(t)]++;
+  });
 }
 
 // Mode table of the given rings: modes (i, j) of each ring in row-major pixel
@@ -300,9 +431,15 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
         if (own[u] && u_ncombo[u] > 0) search(u);
     });
   }
-  // tiles and groups
-  for (int u = 0; u < d.n_used; ++u) {
-    if (!own[u]) continue;
+  // tiles and groups, per triplet on up to 16 host threads (each triplet's
+  // tiles in local lists, joined in triplet order below: the same tables as
+  // one pass in triplet order)
+  std::vector<std::vector<TriTile>> u_tiles(d.n_used);
+  std::vector<std::vector<int32_t>> u_tc(d.n_used);
+  std::vector<char> too_big(d.n_used, 0);
+  auto tile_triplet = [&](int u) {
+    std::vector<TriTile> &tiles = u_tiles[u];
+    std::vector<int32_t> &tile_combo = u_tc[u];
     int cf = u_cfirst[u], nc = u_ncombo[u];
     const int p3min = org[u].p3min, o1 = org[u].o1, o3 = org[u].o3;
     std::vector<Slot> slots(nc);
@@ -351,11 +488,27 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
         tiles.back() = tl;
         gr.ntiles++;
       }
-      if (gr.ntiles > TRI_WARPS) {
+      if (gr.ntiles > TRI_WARPS) too_big[u] = 1;
+      groups[u].push_back(gr);
+    }
+  };
+  {
+    const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    host_parallel(nt, [&](int k) {
+      for (int u = k; u < d.n_used; u += nt)
+        if (own[u]) tile_triplet(u);
+    });
+    for (int u = 0; u < d.n_used; ++u) {
+      if (too_big[u]) {
         set_detail("tile group larger than a CTA");
         return BEAM_EINVAL;
       }
-      groups[u].push_back(gr);
+      const int base = (int)tiles.size();
+      for (Group &gr : groups[u]) gr.tile0 += base;
+      tiles.insert(tiles.end(), u_tiles[u].begin(), u_tiles[u].end());
+      tile_combo.insert(tile_combo.end(), u_tc[u].begin(), u_tc[u].end());
+      std::vector<TriTile>().swap(u_tiles[u]);
+      std::vector<int32_t>().swap(u_tc[u]);
     }
   }
   // splits, pieces, chunks, items
@@ -545,6 +698,10 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   });
   std::vector<TriItem> sorted(items.size());
   for (size_t k = 0; k < order.size(); ++k) sorted[k] = items[order[k]];
+  // the persistent kernel's order: every item by decreasing work (ties: class order)
+  std::vector<int32_t> q_order(items.size());
+  std::iota(q_order.begin(), q_order.end(), 0);
+  std::stable_sort(q_order.begin(), q_order.end(), [&](int x, int y) { return work[order[x]] > work[order[y]]; });
   size_t elem = (A == 1) ? 16 : 8;
   size_t budget = p->ctx->smem_optin > 4096 ? p->ctx->smem_optin - 4096 : 48 * 1024;
   for (int n = 0; n <= TRI_WARPS + 1; ++n) d.class_first[n] = 0;
@@ -570,6 +727,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   BEAM_TRY(upload(p, &d.chunks, chunks));
   BEAM_TRY(upload(p, &d.pieces, pieces));
   BEAM_TRY(upload(p, &d.items, sorted));
+  BEAM_TRY(upload(p, &d.q_order, q_order));
   // per-chunk copy descriptors; the list, chunk and piece tables are then no longer needed
   BEAM_TRY(dev_alloc(p, &d.descs, (size_t)d.n_chunks));
   if (d.n_chunks) {
@@ -593,6 +751,11 @@ int build_plan_tables(beam_gpu_plan *p) {
   DevPlan &d = p->d;
   const long NN = g.NN, Nr = g.Nr;
   const long long ntri = g.ntri;
+  auto now = [] { return std::chrono::steady_clock::now(); };
+  auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+    return (float)std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  const auto t0 = now();
 
   // rings and planes in use
   std::vector<char> ring_on(Nr, 0);
@@ -649,37 +812,31 @@ int build_plan_tables(beam_gpu_plan *p) {
     }
   d.n_used = (int)p->used_rp.size();
   d.n_combo = ntri;
-  std::vector<int32_t> u_cfirst(d.n_used + 1, 0), u_ncombo(d.n_used, 0);
-  for (long long t = 0; t < ntri; ++t) u_ncombo[u_of_rp[g.t_rp[t]]]++;
-  for (int u = 0; u < d.n_used; ++u) u_cfirst[u + 1] = u_cfirst[u] + u_ncombo[u];
+  std::vector<int32_t> u_cfirst, u_ncombo(d.n_used, 0);
   std::vector<int32_t> combo_p1(ntri), combo_p2(ntri), combo_u(ntri), combo_tid(ntri);
   {
-    std::vector<int32_t> fill(u_cfirst.begin(), u_cfirst.end() - 1);
-    for (long long t = 0; t < ntri; ++t) {
-      int u = u_of_rp[g.t_rp[t]];
-      int c = fill[u]++;
-      combo_p1[c] = g.t_p1[t];
-      combo_p2[c] = g.t_p2[t];
-      combo_u[c] = u;
-      combo_tid[c] = (int32_t)t;
-    }
+    // combos grouped by triplet, loop order within a triplet
+    std::vector<int32_t> at;
+    stable_bucket_sort(ntri, d.n_used, [&](long long t) { return u_of_rp[g.t_rp[t]]; }, at, u_cfirst);
+    for (int u = 0; u < d.n_used; ++u) u_ncombo[u] = u_cfirst[u + 1] - u_cfirst[u];
+    const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    host_parallel(nt, [&](int k) {
+      for (long long t = ntri * k / nt; t < ntri * (k + 1) / nt; ++t) {
+        const int c = at[t];
+        combo_p1[c] = g.t_p1[t];
+        combo_p2[c] = g.t_p2[t];
+        combo_u[c] = u_of_rp[g.t_rp[t]];
+        combo_tid[c] = (int32_t)t;
+      }
+    });
   }
 
   // bin order (stable in loop order)
   d.n_bins = g.n_k1bin * g.n_mtbin * g.n_mtbin;
-  std::vector<int32_t> bin_first(d.n_bins + 1, 0);
-  for (long long t = 0; t < ntri; ++t) bin_first[g.t_bin[t] + 1]++;
-  for (int b = 0; b < d.n_bins; ++b) bin_first[b + 1] += bin_first[b];
-  p->bin_pos.assign(ntri, 0);
+  std::vector<int32_t> bin_first;
+  stable_bucket_sort(ntri, d.n_bins, [&](long long t) { return g.t_bin[t]; }, p->bin_pos, bin_first);
   p->loop_of_bin.assign(ntri, 0);
-  {
-    std::vector<int32_t> fill(bin_first.begin(), bin_first.end() - 1);
-    for (long long t = 0; t < ntri; ++t) {
-      int at = fill[g.t_bin[t]]++;
-      p->bin_pos[t] = at;
-      p->loop_of_bin[at] = (int32_t)t;
-    }
-  }
+  for (long long t = 0; t < ntri; ++t) p->loop_of_bin[p->bin_pos[t]] = (int32_t)t;
   std::vector<int32_t> combo_out(ntri);
   for (long long c = 0; c < ntri; ++c) combo_out[c] = p->bin_pos[combo_tid[c]];
 
@@ -689,14 +846,10 @@ int build_plan_tables(beam_gpu_plan *p) {
   // fewer times. At NN=384 this lengthens the mean run (weighted by work) from
   // 17 to 50 triangles. Both orientations are counted on the GPU.
   std::vector<char> u_swap(d.n_used, 0);
+  std::vector<int> chosen;  // the counts of the chosen orientation, triplet by triplet
   {
-    std::vector<char> all(d.n_used, 1);
-    std::vector<long long> f2, f3;
     std::vector<int> c2, c3;
-    BEAM_TRY(enumerate_in_plane(p, p->used_rp, p->ring_first, d.mode_ij, d.ringmap, nullptr, f2, nullptr, nullptr,
-                                &c2, nullptr));
-    BEAM_TRY(enumerate_in_plane(p, p->used_rp, p->ring_first, d.mode_ij, d.ringmap, nullptr, f3, nullptr, nullptr,
-                                &c3, &all));
+    BEAM_TRY(count_both_orientations(p, d.mode_ij, d.ringmap, d.pixlocal, c2, c3));
     size_t a2 = 0, a3 = 0;
     for (int u = 0; u < d.n_used; ++u) {
       const int rp = p->used_rp[u], r2 = g.rp[3 * rp + 1], r3 = g.rp[3 * rp + 2];
@@ -705,6 +858,9 @@ int build_plan_tables(beam_gpu_plan *p) {
       for (int k = 0; k < n2; ++k) runs2 += (c2[a2 + k] > 0);
       for (int k = 0; k < n3; ++k) runs3 += (c3[a3 + k] > 0);
       u_swap[u] = runs3 < runs2;
+      const std::vector<int> &src = u_swap[u] ? c3 : c2;
+      const size_t at = u_swap[u] ? a3 : a2;
+      chosen.insert(chosen.end(), src.begin() + at, src.begin() + at + (u_swap[u] ? n3 : n2));
       a2 += n2;
       a3 += n3;
     }
@@ -717,18 +873,23 @@ int build_plan_tables(beam_gpu_plan *p) {
   // in-plane triangle lists (GPU), run-leg-major: k2cnt holds each run's length
   std::vector<int> k2cnt;
   BEAM_TRY(enumerate_in_plane(p, p->used_rp, p->ring_first, d.mode_ij, d.ringmap, d.pixlocal, p->tri_first,
-                              &d.tri_list, &d.n_terms, &k2cnt, &u_swap));
+                              &d.tri_list, &d.n_terms, &k2cnt, &u_swap, &chosen));
 
   // epilogue tables in bin order
   std::vector<double> ep_px(ntri), ep_pz(ntri), ep_ana(ntri);
   std::vector<int32_t> ep_cnt(ntri);
-  for (long long i = 0; i < ntri; ++i) {
-    long long t = p->loop_of_bin[i];
-    ep_px[i] = g.t_px[t];
-    ep_pz[i] = g.t_pz[t];
-    ep_ana[i] = g.t_ana[t];
-    int u = u_of_rp[g.t_rp[t]];
-    ep_cnt[i] = (int32_t)(p->tri_first[u + 1] - p->tri_first[u]);
+  {
+    const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    host_parallel(nt, [&](int k) {
+      for (long long i = ntri * k / nt; i < ntri * (k + 1) / nt; ++i) {
+        long long t = p->loop_of_bin[i];
+        ep_px[i] = g.t_px[t];
+        ep_pz[i] = g.t_pz[t];
+        ep_ana[i] = g.t_ana[t];
+        int u = u_of_rp[g.t_rp[t]];
+        ep_cnt[i] = (int32_t)(p->tri_first[u + 1] - p->tri_first[u]);
+      }
+    });
   }
 
   // ring triplets this shard sums: longest-processing-time assignment by
@@ -744,9 +905,13 @@ int build_plan_tables(beam_gpu_plan *p) {
   }
 
   // work decomposition of the triangle-sum kernel
+  const auto t1 = now();
+  p->build_ms[1] = ms(t0, t1);
   std::vector<int32_t> u_nsplit;
   std::vector<long long> u_part;
   BEAM_TRY(build_work(p, u_cfirst, u_ncombo, combo_p1, combo_p2, k2cnt, own, u_swap, A, u_nsplit, u_part));
+  const auto t2 = now();
+  p->build_ms[2] = ms(t1, t2);
   d.n_part = u_part[d.n_used];
   u_part.pop_back();
   u_cfirst.pop_back();
@@ -779,6 +944,7 @@ int build_plan_tables(beam_gpu_plan *p) {
   BEAM_TRY(upload(p, &d.ep_cnt, ep_cnt));
 
   d.elem = (p->cfg.precision == BEAM_PREC_MIXED) ? sizeof(float2) : sizeof(double2);
+  p->build_ms[3] = ms(t2, now());
   return BEAM_OK;
 }
 
@@ -786,7 +952,7 @@ void free_plan_tables(beam_gpu_plan *p) {
   DevPlan &d = p->d;
   void *ptrs[] = {d.mode_ij,  d.mode_neg, d.ringmap, d.pixlocal,   d.tri_list, d.combo_u, d.combo_out,
                   d.u_cfirst, d.u_ncombo, d.u_nsplit, d.u_part,    d.tiles,    d.tile_combo, d.chunks,
-                  d.pieces,   d.descs,    d.items,    d.bin_first, d.ep_px,    d.ep_pz,   d.ep_cnt,
+                  d.pieces,   d.descs,    d.items,    d.q_order,   d.bin_first, d.ep_px,  d.ep_pz,   d.ep_cnt,
                   d.ep_chunk_first, d.bin_chunk, d.ep_ana};
   for (void *q : ptrs)
     if (q) cudaFree(q);

@@ -282,7 +282,7 @@ static int slot_alloc(beam_gpu_plan *p, RunSlot *s) {
   BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->bins, z.bins));
   BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->bin_count, z.count));
   BEAM_TRY(dev_alloc(&s->bytes, (unsigned char **)&s->ep_part, z.ep));
-  BEAM_TRY(dev_alloc(&s->bytes, &s->status, 1));
+  BEAM_TRY(dev_alloc(&s->bytes, &s->status, 2));  // status word, persistent kernel's work counter
   BEAM_CUDA(cudaMallocHost(&s->h_staging, std::max<size_t>(16, z.staging)));
   BEAM_CUDA(cudaMallocHost((void **)&s->h_src, z.src));
   BEAM_CUDA(cudaMallocHost(&s->h_bins, std::max<size_t>(16, z.bins)));

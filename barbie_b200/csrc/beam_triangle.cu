@@ -50,7 +50,9 @@ struct TriArgs {
   double *part;
   int *status;
   int stage;              // complex values per stage
-  int nreal;              // realizations per launch (blockIdx.y)
+  int nreal;              // realizations per launch
+  int real;               // realization of the item being summed
+  int stage_of[TRI_WARPS + 1];  // stage size of each tile count (the persistent kernel's items)
   long long s_stride;     // complex values of S per realization
   long long part_stride;  // partial sums per realization
 };
@@ -108,10 +110,10 @@ __device__ __forceinline__ bool tri_wait_chunk(const TriArgs &a, uint64_t *full,
   return true;
 }
 
-// Partial-sum slots of this CTA's item (split `it.split`) for realization blockIdx.y.
+// Partial-sum slots of this CTA's item (split `it.split`) for realization a.real.
 __device__ __forceinline__ double *tri_out(const TriArgs &a, const TriItem &it) {
   const int nc = a.u_ncombo[it.u];
-  return a.part + (long long)blockIdx.y * a.part_stride + a.u_part[it.u] + (long long)it.split * nc -
+  return a.part + (long long)a.real * a.part_stride + a.u_part[it.u] + (long long)it.split * nc -
          a.u_cfirst[it.u];
 }
 
@@ -511,14 +513,74 @@ struct TriBounds<float2> {
   static constexpr int threads = 32 * (fma_max_cons_warps() + 1), blocks = 3;
 };
 
+// Consumer warps of a CTA for an item of n tiles: one per tile on the FP64
+// tensor cores and for the FP32 consumer of one or two tiles, one per pair of
+// tiles for the packed FP32 consumer of more.
+template <typename C>
+__host__ __device__ inline int cons_warps(int n) {
+  return std::is_same<C, double2>::value ? n : fma_cons_warps(n);
+}
+
+// One work item (its tiles over its chunks, realization a.real) on this CTA:
+// warp `producer` streams the chunks into the stage ring, warps [0, ncons)
+// consume them, any other warp takes no part. The caller has initialised the
+// barriers (empty[] counting ncons arrivals).
+template <typename C>
+__device__ __forceinline__ void tri_run_item(const TriArgs &a, const TriItem &it, unsigned char *smem_raw,
+                                             uint64_t *full, uint64_t *empty, volatile int *s_fail, int producer,
+                                             int ncons) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  C *stages = reinterpret_cast<C *>(smem_raw);
+  const C *S = static_cast<const C *>(a.S) + (size_t)a.real * a.s_stride;
+  const int nch = it.ch1 - it.ch0;
+
+  if (warp == producer) {
+    // ------------------------------------------------------------ producer
+    int issued = 0;
+    bool failed = false;
+    TriMeta meta = nch > 0 ? tri_meta(a, it.ch0) : TriMeta{0, 0u, 0};
+    for (int c = 0; c < nch; ++c) {
+      const int s = c % TRI_STAGES;
+      if (c >= TRI_STAGES &&
+          (*s_fail || !mbar_wait_bounded(smem_addr(&empty[s]), (uint32_t)(((c / TRI_STAGES) - 1) & 1)))) {
+        failed = true;
+        break;
+      }
+      const TriMeta cur = meta;
+      if (c + 1 < nch) meta = tri_meta(a, it.ch0 + c + 1);
+      tri_issue<C>(a, it, S, stages + s * a.stage, smem_addr(&full[s]), cur);
+      issued = c + 1;
+    }
+    if (failed) {
+      *s_fail = 1;
+      if (lane == 0) atomicOr(a.status, DEV_TIMEOUT);
+      // let the copies in flight (the last TRI_STAGES issued) land before the
+      // CTA's shared memory can be released or restaged
+      for (int c = issued - TRI_STAGES > 0 ? issued - TRI_STAGES : 0; c < issued; ++c)
+        mbar_wait_bounded(smem_addr(&full[c % TRI_STAGES]), (uint32_t)((c / TRI_STAGES) & 1));
+    }
+    return;
+  }
+  if (warp >= ncons) return;
+
+  // -------------------------------------------------------------- consumer
+  if constexpr (std::is_same<C, double2>::value)
+    tri_consume_dmma(a, it, stages, full, empty, s_fail, warp, lane, nch);
+  else if (!fma_pairs_tiles(it.ntiles))
+    tri_consume_fma_tile<C>(a, it, stages, full, empty, s_fail, warp, lane, nch);
+  else
+    tri_consume_fma<C>(a, it, stages, full, empty, s_fail, warp, lane, nch);
+}
+
+// One CTA per item of one tile class (blockIdx.x) and realization (blockIdx.y);
+// the CTA has cons_warps(n) consumer warps and the producer warp last.
 template <typename C>
 __global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks) k_triangle(TriArgs a) {
-  typedef typename TriAcc<C>::t acc_t;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[TRI_STAGES], empty[TRI_STAGES];
   __shared__ volatile int s_fail;
-  const TriItem it = a.items[blockIdx.x];  // realization blockIdx.y
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const TriItem it = a.items[blockIdx.x];
+  const int tid = threadIdx.x;
   const int ncons = (blockDim.x >> 5) - 1;  // consumer warps (cons_warps); warp ncons produces
   if (tid == 0) {
     for (int s = 0; s < TRI_STAGES; ++s) {
@@ -529,45 +591,53 @@ __global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks) k
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  C *stages = reinterpret_cast<C *>(smem_raw);
-  const C *S = static_cast<const C *>(a.S) + (size_t)blockIdx.y * a.s_stride;
-  const int nch = it.ch1 - it.ch0;
+  TriArgs b = a;
+  b.real = blockIdx.y;
+  tri_run_item<C>(b, it, smem_raw, full, empty, &s_fail, ncons, ncons);
+}
 
-  if (warp == ncons) {
-    // ------------------------------------------------------------ producer
-    int issued = 0;
-    bool failed = false;
-    TriMeta meta = nch > 0 ? tri_meta(a, it.ch0) : TriMeta{0, 0u, 0};
-    for (int c = 0; c < nch; ++c) {
-      const int s = c % TRI_STAGES;
-      if (c >= TRI_STAGES &&
-          (s_fail || !mbar_wait_bounded(smem_addr(&empty[s]), (uint32_t)(((c / TRI_STAGES) - 1) & 1)))) {
-        failed = true;
-        break;
+// Persistent form: every item of every tile class and every realization in one
+// launch. A CTA (the largest class's shape: its consumer warps plus the
+// producer warp last) takes work units from a device counter -- unit w is
+// item order[w / nreal] (items in decreasing order of work) for realization
+// w % nreal -- sets its barriers up for the unit's consumer count, sums it and
+// takes the next, until the units run out. The counter must be zero at launch.
+template <typename C>
+__global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks)
+    k_triangle_q(TriArgs a, const int32_t *__restrict__ order, int n_units, int *counter) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t full[TRI_STAGES], empty[TRI_STAGES];
+  __shared__ volatile int s_fail;
+  __shared__ int s_unit;
+  const int tid = threadIdx.x;
+  const int producer = (blockDim.x >> 5) - 1;
+  if (tid == 0) s_fail = 0;
+  bool inited = false;
+  for (;;) {
+    if (tid == 0) s_unit = atomicAdd(counter, 1);
+    __syncthreads();  // every warp is done with the previous unit
+    const int w = s_unit;
+    if (w >= n_units || s_fail) break;
+    const TriItem it = a.items[order[w / a.nreal]];
+    const int ncons = cons_warps<C>(it.ntiles);
+    if (tid == 0) {
+      for (int s = 0; s < TRI_STAGES; ++s) {
+        if (inited) {
+          mbar_inval(smem_addr(&full[s]));
+          mbar_inval(smem_addr(&empty[s]));
+        }
+        mbar_init(smem_addr(&full[s]), 1);
+        mbar_init(smem_addr(&empty[s]), ncons);
       }
-      const TriMeta cur = meta;
-      if (c + 1 < nch) meta = tri_meta(a, it.ch0 + c + 1);
-      tri_issue<C>(a, it, S, stages + s * a.stage, smem_addr(&full[s]), cur);
-      issued = c + 1;
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (failed) {
-      s_fail = 1;
-      if (lane == 0) atomicOr(a.status, DEV_TIMEOUT);
-      // let the copies in flight (the last TRI_STAGES issued) land before the
-      // CTA's shared memory can be released
-      for (int c = issued - TRI_STAGES > 0 ? issued - TRI_STAGES : 0; c < issued; ++c)
-        mbar_wait_bounded(smem_addr(&full[c % TRI_STAGES]), (uint32_t)((c / TRI_STAGES) & 1));
-    }
-    return;
+    inited = true;
+    __syncthreads();  // barriers ready; s_unit read by every thread
+    TriArgs b = a;
+    b.real = w % a.nreal;
+    b.stage = a.stage_of[it.ntiles];
+    tri_run_item<C>(b, it, smem_raw, full, empty, &s_fail, producer, ncons);
   }
-
-  // -------------------------------------------------------------- consumer
-  if constexpr (std::is_same<C, double2>::value)
-    tri_consume_dmma(a, it, stages, full, empty, &s_fail, warp, lane, nch);
-  else if (!fma_pairs_tiles(it.ntiles))
-    tri_consume_fma_tile<C>(a, it, stages, full, empty, &s_fail, warp, lane, nch);
-  else
-    tri_consume_fma<C>(a, it, stages, full, empty, &s_fail, warp, lane, nch);
 }
 
 // Sum the splits of each combo in split order, scale by NN^2 and store the
@@ -589,14 +659,6 @@ __global__ void k_reduce(long long n_combo, const int32_t *__restrict__ combo_u,
   B[combo_out[c]] = nn2 * s;
 }
 
-// Consumer warps of a CTA with n tiles: one per tile on the FP64 tensor
-// cores and for the FP32 consumer of one or two tiles, one per pair of tiles
-// for the packed FP32 consumer of more.
-template <typename C>
-static int cons_warps(int n) {
-  return std::is_same<C, double2>::value ? n : fma_cons_warps(n);
-}
-
 template <typename C>
 static size_t tri_smem(int stage, int ntiles) {
   (void)ntiles;
@@ -612,6 +674,9 @@ static int allow_optin(size_t smem_optin) {
   BEAM_CUDA(cudaFuncGetAttributes(&fa, k_triangle<C>));
   int dyn = (int)(smem_optin > fa.sharedSizeBytes ? smem_optin - fa.sharedSizeBytes : 0);
   BEAM_CUDA(cudaFuncSetAttribute(k_triangle<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+  BEAM_CUDA(cudaFuncGetAttributes(&fa, k_triangle_q<C>));
+  dyn = (int)(smem_optin > fa.sharedSizeBytes ? smem_optin - fa.sharedSizeBytes : 0);
+  BEAM_CUDA(cudaFuncSetAttribute(k_triangle_q<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
   return BEAM_OK;
 }
 
@@ -648,6 +713,41 @@ static int launch_classes(beam_gpu_plan *p, RunSlot *s, TriArgs a) {
   return BEAM_OK;
 }
 
+// All classes and realizations in one launch of the persistent kernel on the
+// slot's stream: the work counter is zeroed first (a memset node in a
+// captured graph), then as many CTAs as fit the device at once take units.
+template <typename C>
+static int launch_persistent(beam_gpu_plan *p, RunSlot *s, TriArgs a) {
+  DevPlan &d = p->d;
+  cudaStream_t st = s->lane->stream;
+  int max_stage = 0;
+  for (int n = 1; n <= TRI_WARPS; ++n) {
+    a.stage_of[n] = d.class_stage[n];
+    max_stage = std::max(max_stage, d.class_stage[n]);
+  }
+  a.stage_of[0] = 0;
+  const size_t smem = tri_smem<C>(max_stage, TRI_WARPS);
+  const int threads = TriBounds<C>::threads;
+  int per_sm = 0;
+  BEAM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_triangle_q<C>, threads, smem));
+  if (per_sm < 1) {
+    set_detail("the persistent triangle kernel does not fit an SM");
+    return BEAM_EINVAL;
+  }
+  const long long units = (long long)d.n_items * a.nreal;
+  if (units > 0x7fffffffLL) {
+    set_detail("too many triangle-sum work units for one persistent launch");
+    return BEAM_EINVAL;
+  }
+  const int grid = (int)std::min<long long>(units, (long long)per_sm * std::max(1, p->ctx->num_sms));
+  int *counter = s->status + 1;
+  BEAM_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+  k_triangle_q<C><<<grid, threads, smem, st>>>(a, d.q_order, (int)units, counter);
+  BEAM_CUDA(cudaGetLastError());
+  s->launches++;
+  return BEAM_OK;
+}
+
 int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n) {
   DevPlan &d = p->d;
   if (d.n_combo == 0) {
@@ -669,13 +769,16 @@ int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n) {
   a.status = s->status;
   a.stage = 0;
   a.nreal = n;
+  a.real = 0;
+  for (int k = 0; k <= TRI_WARPS; ++k) a.stage_of[k] = 0;
   a.s_stride = (long long)d.n_modes * d.W;
   a.part_stride = d.n_part;
   mark(s, 1);
+  const bool persistent = p->tri_launch == BEAM_LAUNCH_PERSISTENT;
   if (d.elem == sizeof(double2))
-    BEAM_TRY(launch_classes<double2>(p, s, a));
+    BEAM_TRY(persistent ? launch_persistent<double2>(p, s, a) : launch_classes<double2>(p, s, a));
   else
-    BEAM_TRY(launch_classes<float2>(p, s, a));
+    BEAM_TRY(persistent ? launch_persistent<float2>(p, s, a) : launch_classes<float2>(p, s, a));
   mark(s, 2);
   double nn2 = (double)p->geom.NN * (double)p->geom.NN;
   dim3 grid((unsigned)((d.n_combo + 255) / 256), (unsigned)n);

@@ -130,9 +130,9 @@ static int eval_triangle(const beam_geom *g, int r1, int r2, int r3, int p1, int
   {
     const double ff = 0.1, beta = 1., Cunits = 2. * M_PI / (g->NN * g->LL);
     double mu_1 = p[0] / k[0], mu_2 = p[1] / k[1], mu_3 = p[2] / k[2];
-    double ana = 2. * ff * (input_ps(Cunits * k[0]) * input_ps(Cunits * k[1]) +
-                            input_ps(Cunits * k[1]) * input_ps(Cunits * k[2]) +
-                            input_ps(Cunits * k[2]) * input_ps(Cunits * k[0]));
+    /* each leg's P(k) once: the same values the reference computes twice */
+    double P0 = input_ps(Cunits * k[0]), P1 = input_ps(Cunits * k[1]), P2 = input_ps(Cunits * k[2]);
+    double ana = 2. * ff * (P0 * P1 + P1 * P2 + P2 * P0);
     e->ana = ana * (1 + beta * mu_1 * mu_1) * (1 + beta * mu_2 * mu_2) * (1 + beta * mu_3 * mu_3);
   }
   int n = g->n_mtbin;
@@ -157,8 +157,24 @@ static void p2_limits(int p1, long Nmax, int r1, int r2, int r3, int *lo, int *h
   }
 }
 
+/* Acceptance alone (barbie.c:285,292): |p3| < Nmax and LL_k1 < K1 < UL_k1,
+ * K1 the largest of the three legs' |K| -- the same sqrt expressions as
+ * eval_triangle, so the same triangles pass. */
+static int accepted(const beam_geom *g, int r1, int r2, int r3, int p1, int p2) {
+  int p3 = -p1 - p2;
+  if (!((p3 < 0 ? -p3 : p3) < g->Nmax)) return 0;
+  const double *a = g->avg;
+  double k1 = sqrt(a[r1] * a[r1] + p1 * p1), k2 = sqrt(a[r2] * a[r2] + p2 * p2), k3 = sqrt(a[r3] * a[r3] + p3 * p3);
+  double K1 = k1 > k2 ? k1 : k2;
+  K1 = K1 > k3 ? K1 : k3;
+  return K1 > g->LL_k1 && K1 < g->UL_k1;
+}
+
 /* The loop is split over p1 (the reference's outer loop) between threads; each
- * p1 first counts, then fills its own slice, so triangles keep loop order. */
+ * p1 first counts, then fills its own slice, so triangles keep loop order.
+ * A leg's |K| = sqrt(avg^2 + p^2) is at least |p|, so no triangle with a plane
+ * |p| >= UL_k1 passes the k1 window: those iterations are counted, not
+ * visited. */
 typedef struct {
   beam_geom *g;
   long *count;       /* [Nmax] accepted per p1 */
@@ -173,16 +189,30 @@ typedef struct {
 static void enumerate_p1(enum_job *job, int p1) {
   beam_geom *g = job->g;
   long n = 0, it = 0, at = job->fill ? job->offset[p1] : 0;
+  const int U = g->UL_k1;
   for (long rp = 0; rp < g->nrp; ++rp) {
     int r1 = g->rp[3 * rp], r2 = g->rp[3 * rp + 1], r3 = g->rp[3 * rp + 2];
     int lo, hi;
     p2_limits(p1, g->Nmax, r1, r2, r3, &lo, &hi);
-    for (int p2 = lo; p2 <= hi; ++p2) {
-      ++it;
+    if (hi >= lo) it += hi - lo + 1;
+    if (p1 >= U) continue;
+    /* |p2| < U and |p1 + p2| < U */
+    int clo = lo > -U + 1 ? lo : -U + 1, chi = hi < U - 1 ? hi : U - 1;
+    if (clo < -U + 1 - p1) clo = -U + 1 - p1;
+    if (chi > U - 1 - p1) chi = U - 1 - p1;
+    for (int p2 = clo; p2 <= chi; ++p2) {
+      if (!job->fill) {
+        n += accepted(g, r1, r2, r3, p1, p2);
+        continue;
+      }
       tri_eval e;
       if (!eval_triangle(g, r1, r2, r3, p1, p2, &e)) continue;
       if (e.bad_bin) job->bad[p1] = 1;
-      if (job->fill) {
+      if (at >= job->offset[p1] + job->count[p1]) { /* the count pass disagreed: never write past p1's slice */
+        job->bad[p1] |= 2;
+        continue;
+      }
+      {
         g->t_rp[at] = (int32_t)rp;
         g->t_p1[at] = p1;
         g->t_p2[at] = p2;
@@ -248,7 +278,6 @@ static int build_triangles(beam_geom *g) {
     job.offset[p] = total;
     total += job.count[p];
     iters += job.iters[p];
-    bad |= job.bad[p];
   }
   int rc = BEAM_OK;
   size_t n = (size_t)(total > 0 ? total : 1);
@@ -266,7 +295,9 @@ static int build_triangles(beam_geom *g) {
     run_pass(&job, nthreads);
     g->ntri = total;
     g->iterations = iters;
-    if (bad) rc = BEAM_EBOUNDS;
+    for (long p = 0; p < Nmax; ++p) bad |= job.bad[p];
+    if (bad & 2) rc = BEAM_EINVAL; /* count and fill passes disagree (not expected) */
+    else if (bad) rc = BEAM_EBOUNDS;
   }
   pthread_mutex_destroy(&job.lock);
   free(job.count); free(job.offset); free(job.iters); free(job.bad);

@@ -258,7 +258,9 @@ def run_ours(args):
     t1 = time.perf_counter()
     plan.run(host_np[0])
     t2 = time.perf_counter()
-    cold = {"plan_create_ms": (t1 - t0) * 1e3, "first_run_ms": (t2 - t1) * 1e3, "total_ms": (t2 - t0) * 1e3}
+    cold = {"plan_create_ms": (t1 - t0) * 1e3, "first_run_ms": (t2 - t1) * 1e3, "total_ms": (t2 - t0) * 1e3,
+            "phases_ms": dict(zip(("geometry", "triangle_lists", "work", "tables", "run_buffers"),
+                                  plan.info["build_ms"]))}
     tuning = {"fp64": tune_plan(plan, args)}
     info = plan.info
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -313,6 +315,13 @@ def run_ours(args):
     e2e_value = world * args.steps / (e2e_total / 1e3) * 3600.0
     h2d = info["n_modes"] * info["n_planes"] * 16
     d2h = info["n_bins"] * (3 * 16 * 8 + 8)
+
+    # the same bispectra with the triangle sums in one persistent launch
+    plan.set_triangle_launch("persistent")
+    timed_loop(plan, dev_fields, args.warmup)
+    p_times, p_tri = timed_loop(plan, dev_fields, args.steps)
+    plan.set_triangle_launch("classes")
+    persistent = {"ms_per_step": float(np.mean(p_times)), "triangle_ms": float(np.mean(p_tri))}
 
     # latency percentiles of single jobs (device-resident and e2e)
     lat = {"p50_ms": float(np.percentile(times, 50)), "p99_ms": float(np.percentile(times, 99)),
@@ -406,11 +415,13 @@ def run_ours(args):
         "serve_mixed_p99_ms": serving["mixed"]["p99_ms"] if serving else None,
         "batched_value": batched["mixed"]["batch_of_16"]["value"] if batched else None,
         "batched_fp64_value": batched["fp64"]["batch_of_16"]["value"] if batched else None,
+        "batched_persistent_value": batched["mixed"]["batch_of_16_persistent"]["value"] if batched else None,
+        "batched_fp64_persistent_value": batched["fp64"]["batch_of_16_persistent"]["value"] if batched else None,
         "cold_start_ms": cold["total_ms"],
         "latency_p50_ms": lat["p50_ms"], "latency_p99_ms": lat["p99_ms"],
     }
     details = {"roofline": roofline, "mixed": mixed, "fp64_vs_oracle": fp64_vs_oracle, "cpu_baseline": cpu,
-               "cold_start": cold, "latency": lat, "wall_s": wall, "batched": batched, "serving": serving,
+               "cold_start": cold, "latency": lat, "persistent_launch": persistent, "wall_s": wall, "batched": batched, "serving": serving,
                "field": field, "autotune": tuning,
                "plan": {"n_triples": info["n_triples"], "n_fourier_terms": info["n_fourier_terms"],
                         "n_run_combos": info["n_run_combos"], "plan_device_bytes": info["device_bytes"]}}
@@ -447,14 +458,19 @@ def run_batched(ctx, args):
         plan = beam.Plan(ctx, B["NN"], B["UL_k1"], B["LL_k1"], B["BW_k1"], Nmax=B["Nmax"], Nr=B["Nr"],
                          n_mtbin=B["n_mtbin"], precision=prec)
         res = {}
-        for label, batch in (("batched", 0), ("batch_of_16", 16)):
-            plan.run_batch(fields, batch=batch)  # warm-up: slots and graphs
-            t = []
-            for _ in range(max(1, args.steps // 3)):
-                t0 = time.perf_counter()
-                plan.run_batch(fields, batch=batch)
-                t.append(time.perf_counter() - t0)
-            res[label] = {"value": len(fields) / min(t) * 3600.0, "seconds_per_call": min(t)}
+        for mode in ("classes", "persistent"):
+            plan.set_triangle_launch(mode)
+            for label, batch in (("batched", 0), ("batch_of_16", 16)):
+                plan.run_batch(fields, batch=batch)  # warm-up: slots and graphs
+                t = []
+                for _ in range(max(1, args.steps // 3)):
+                    t0 = time.perf_counter()
+                    plan.run_batch(fields, batch=batch)
+                    t.append(time.perf_counter() - t0)
+                key = label if mode == "classes" else f"{label}_persistent"
+                res[key] = {"value": len(fields) / min(t) * 3600.0, "seconds_per_call": min(t),
+                            "launches_per_batch": plan.refresh_info()["launches_last_run"]}
+        plan.set_triangle_launch("classes")
         for f in pool[:2]:
             plan.run(f)
         t0 = time.perf_counter()

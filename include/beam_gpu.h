@@ -128,6 +128,9 @@ typedef struct beam_plan_info {
   long n_run_combos;      /* sum over accepted triangles of the runs of their triplet's in-plane list
                              (triangles sharing the mode of the leg whose plane is -p1 - p(tile), whose
                              product with the run's accumulated outer product is formed once per run) */
+  float build_ms[5];      /* host wall time of the plan's creation, ms: [0] geometry (rings, triplets,
+                             accepted triangles), [1] mode tables and in-plane triangle lists (GPU),
+                             [2] work decomposition, [3] remaining device tables, [4] run buffers */
 } beam_plan_info;
 
 /* Library / device setup. Replaces the fftw_init_threads / plan_with_nthreads
@@ -169,6 +172,20 @@ BEAM_API int beam_gpu_run(beam_gpu_plan *plan, const double *r2c, int r2c_on_dev
 BEAM_API int beam_gpu_run_batch(beam_gpu_plan *plan, const double *const *r2c, int n, beam_result *res);
 BEAM_API int beam_gpu_run_batch_ex(beam_gpu_plan *plan, const double *const *r2c, int n, beam_result *res,
                                    int batch);
+
+/* How the plan launches its triangle sums (no counterpart in the reference,
+ * whose triangle loop is one serial loop, barbie.c:247-365):
+ *   BEAM_LAUNCH_CLASSES     one launch per tile class (CTA shape), on side
+ *                           streams that overlap (the default);
+ *   BEAM_LAUNCH_PERSISTENT  one persistent launch over every item of every
+ *                           class and every realization of the run or batch:
+ *                           CTAs of the largest class's shape take work units
+ *                           from a device counter, largest first.
+ * Results are bit-identical either way (every unit sums the same triangles in
+ * the same order). Changing the mode drops the plan's captured batch graphs. */
+#define BEAM_LAUNCH_CLASSES 0
+#define BEAM_LAUNCH_PERSISTENT 1
+BEAM_API int beam_gpu_plan_set_triangle_launch(beam_gpu_plan *plan, int mode);
 
 /* calCR (funcs.c:328-424): closed ring triplets in the reference's order as
  * records {r1, r2, r3, Num} with Num = NN^2 * (exact triangle count) -- the

@@ -107,3 +107,26 @@ def test_launch_count_is_reported(beamlib, ctx):
     # mode build + 1..7 triangle-sum classes + split reduction + 2 epilogue passes
     assert 5 <= n <= 11
     plan.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_launch_equals_class_launches(beamlib, ctx, precision):
+    """One persistent launch of every tile class and realization gives the bins
+    of the per-class launches bit for bit, single runs and batches (the same
+    units sum the same triangles in the same order), and switching the mode back
+    and forth recaptures the batch graphs."""
+    name = "nn256_cfg2"
+    plan = make_plan(beamlib, ctx, name, precision=precision)
+    fields = fields_for(name, range(21, 24))
+    want = [plan.run(f) for f in fields]
+    want_batch = plan.run_batch(fields, batch=2)
+    plan.set_triangle_launch("persistent")
+    for f, w in zip(fields, want):
+        assert_same(plan.run(f), w)
+    for g, w in zip(plan.run_batch(fields, batch=2), want_batch):
+        assert_same(g, w)
+    assert plan.refresh_info()["launches_last_run"] < 8  # mode build, one triangle launch, reduction, epilogue
+    plan.set_triangle_launch("classes")
+    for g, w in zip(plan.run_batch(fields, batch=2), want_batch):
+        assert_same(g, w)
+    plan.close()

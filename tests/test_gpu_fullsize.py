@@ -106,3 +106,18 @@ def test_mixed_error_against_fp64(plans, field):
     assert np.median(rel) <= 1e-6
     assert np.mean(rel <= 1e-5) >= 0.98
     assert rel.max() <= 1e-2
+
+
+@pytest.mark.xfail(strict=True, reason="the FP32 path's maximum error per (l, m, bin) at NN=384 is ~1e-3, not the "
+                                       "north star's 1e-5: bins whose value is small beside their scatter turn the "
+                                       "FP32 rounding of the triangle sums into relative errors above 1e-5")
+def test_mixed_meets_the_1e_5_bar_on_every_bin(plans, field):
+    """The north star's bar for the mixed path: every printed (l, m, bin) within
+    1e-5 of FP64. Kept as a strict expected failure so the unmet bar stays in the
+    test record; it turns into a failure the day the mixed path meets it."""
+    f = plans["fp64"].run(field)
+    m = plans["mixed"].run(field)
+    ok = (f["norm"][..., 0] > 0.1)[..., None] & np.isfinite(f["out"]) & (f["out"] != 0)
+    ok = np.broadcast_to(ok, f["out"].shape)
+    rel = np.abs(m["out"][ok] - f["out"][ok]) / np.abs(f["out"][ok])
+    assert rel.max() <= 1e-5

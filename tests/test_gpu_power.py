@@ -83,3 +83,29 @@ def test_calpow_mom_drop_in(tmp_path):
     assert np.all(np.abs(mine - ref) <= 6e-7 * np.abs(ref))  # %e keeps 7 significant digits
     bad = subprocess.run([exe, str(NN)], cwd=tmp_path, capture_output=True, text=True)
     assert bad.returncode == 1 and "Usage" in bad.stdout
+
+
+def test_repeated_calls_with_kept_geometry_give_the_same_bits(beamlib, oracle):
+    """The first call with a given (NN, Nbin) forms every sum from the modes and
+    keeps the geometry; later calls read it and form only the field's sums, in
+    the same order: the same bits, for another field too, and again after a
+    call with other sizes replaced the kept geometry."""
+    from barbie_b200.synth import realization_seed, synth_field
+    ctx = beamlib.Context(0)
+    name = "nn96_r20"
+    NN = GOLDEN_CASES[name][0]
+    f, g = golden_field(name), synth_field(NN, realization_seed(9))
+    first = beamlib.power_multipoles(ctx, f, NN, LL=0.56, Nbin=10)  # forms everything, keeps the geometry
+    second = beamlib.power_multipoles(ctx, f, NN, LL=0.56, Nbin=10)  # from the kept geometry
+    other = beamlib.power_multipoles(ctx, g, NN, LL=0.56, Nbin=10)
+    beamlib.power_multipoles(ctx, golden_field("nn64_cfg1"), 64, LL=0.56, Nbin=10)  # other sizes replace it
+    again = beamlib.power_multipoles(ctx, f, NN, LL=0.56, Nbin=10)
+    for col in COLS:
+        assert np.array_equal(first[col], second[col]), col
+        assert np.array_equal(first[col], again[col]), col
+    ctx2 = beamlib.Context(0)  # a fresh context forms the other field's sums from its modes
+    fresh = beamlib.power_multipoles(ctx2, g, NN, LL=0.56, Nbin=10)
+    for col in COLS:
+        assert np.array_equal(other[col], fresh[col]), col
+    ctx2.close()
+    ctx.close()
