@@ -238,6 +238,7 @@ class Plan:
         self.n_k1bin = info.n_k1bin
         self.shape = (info.n_k1bin, n_mtbin, n_mtbin, NPOLES)
         self.NN = NN
+        self.precision = precision
 
     def close(self) -> None:
         if getattr(self, "_h", None):

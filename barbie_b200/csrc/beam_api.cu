@@ -135,6 +135,9 @@ int beam_gpu_plan_create(beam_gpu_ctx *ctx, const beam_cfg *cfg, beam_gpu_plan *
   p->ctx = ctx;
   p->cfg = *cfg;
   p->cfg.shard_count = shards;
+  // first split cap of the triangle lists: the autotuner's best at NN=384 for
+  // each path (FP64 1024, mixed 512 triangles per CTA)
+  p->tau0 = cfg->precision == BEAM_PREC_FP64 ? 2 * TRI_TAU_MAX : TRI_TAU_MAX;
   auto now = [] { return std::chrono::steady_clock::now(); };
   auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
     return (float)std::chrono::duration<double, std::milli>(b - a).count();

@@ -130,7 +130,7 @@ struct TriDesc {
   int pad;
 };
 static_assert(sizeof(TriDesc) % 16 == 0 && TRI_CHUNK <= 31 && TRI_PIECES <= 4, "TriDesc layout");
-constexpr int TRI_TAU_MAX = 512;  // most in-plane triangles walked by one CTA
+constexpr int TRI_TAU_MAX = 512;  // first cap on the in-plane triangles one CTA walks (mixed; FP64 twice)
 
 // The mixed path's mode rows are blocked by 4 columns: block b of a row holds
 // the real parts of columns 4b..4b+3, then their imaginary parts (8 floats).
@@ -216,7 +216,8 @@ struct Lane {
   cudaStream_t side[TRI_WARPS] = {};
   cudaEvent_t fork = nullptr, join[TRI_WARPS] = {};
 };
-int lane_create(Lane *l);
+// priority: the streams' CUDA priority (0 = default; lower is more urgent)
+int lane_create(Lane *l, int priority = 0);
 void lane_destroy(Lane *l);
 
 // Per-run buffers for up to `cap` realizations of one plan, processed together
@@ -319,7 +320,7 @@ void free_plan_tables(beam_gpu_plan *p);
 int count_closed_triangles(beam_gpu_plan *p, std::vector<long long> &counts);
 // run slots (beam_run.cu); lane == nullptr gives the slot a lane of its own
 size_t slot_bytes(const beam_gpu_plan *p, int cap);
-int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out);
+int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out, int priority = 0);
 void slot_destroy(RunSlot *s);
 // per-realization steps on a slot, for realizations [0, n) (beam_run.cu)
 void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c, int m0 = 0, int m1 = -1);

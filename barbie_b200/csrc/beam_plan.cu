@@ -520,7 +520,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   // work per SM) and by list length (no CTA walks more than about tau_max
   // triangles: a CTA's time grows with its list, not its tiles). Each split
   // keeps a partial sum per combo, so tau_max starts at the plan's tau0
-  // (TRI_TAU_MAX unless tuned) and doubles while the partial sums would pass
+  // (TRI_TAU_MAX mixed, twice that FP64, unless tuned) and doubles while the partial sums would pass
   // max(PART_PER_COMBO x combos, PART_MIN) slots per realization.
   constexpr long long PART_PER_COMBO = 4, PART_MIN = 64LL << 20;
   std::vector<long long> nruns(d.n_used, 0);

@@ -204,10 +204,10 @@ __global__ void k_ep_bins(const int32_t *__restrict__ bin_chunk, int n_bins, int
 }
 
 // ------------------------------------------------------------ host drivers
-int lane_create(Lane *l) {
-  cudaError_t e = cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking);
+int lane_create(Lane *l, int priority) {
+  cudaError_t e = cudaStreamCreateWithPriority(&l->stream, cudaStreamNonBlocking, priority);
   for (int k = 0; k < TRI_WARPS && e == cudaSuccess; ++k) {
-    e = cudaStreamCreateWithFlags(&l->side[k], cudaStreamNonBlocking);
+    e = cudaStreamCreateWithPriority(&l->side[k], cudaStreamNonBlocking, priority);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l->join[k], cudaEventDisableTiming);
   }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l->fork, cudaEventDisableTiming);
@@ -305,7 +305,7 @@ static int slot_alloc(beam_gpu_plan *p, RunSlot *s) {
   return BEAM_OK;
 }
 
-int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out) {
+int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out, int priority) {
   *out = nullptr;
   if (cap < 1 || cap > 65535) {
     set_detail("slot capacity must be 1..65535 realizations");
@@ -318,7 +318,7 @@ int slot_create(beam_gpu_plan *p, int cap, Lane *lane, RunSlot **out) {
   if (lane) {
     s->lane = lane;
   } else {
-    rc = lane_create(&s->own);
+    rc = lane_create(&s->own, priority);
     s->lane = &s->own;
   }
   if (rc == BEAM_OK) rc = slot_alloc(p, s);

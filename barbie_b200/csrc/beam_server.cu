@@ -13,7 +13,12 @@
 //     waits for it;
 //   * a job runs as the slot's captured graph (H2D of the gathered mode rows,
 //     kernels, D2H of the bins), so jobs on different slots overlap on the GPU;
-//     the dispatcher polls each slot's `done` event to retire it.
+//     the dispatcher polls each slot's `done` event to retire it;
+//   * priority by size: a plan's slots get streams whose CUDA priority falls
+//     with the plan's work (one level per decade of closed-triangle terms
+//     above 1e8), so as the CTAs of a large job retire, those of a small job
+//     that arrived meanwhile are scheduled first and it does not wait for the
+//     large one to drain.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -59,6 +64,7 @@ CfgKey key_of(const beam_cfg &c) {
 struct PlanEntry {
   CfgKey key;
   beam_gpu_plan *plan = nullptr;
+  int priority = 0;         // CUDA stream priority of the plan's job slots
   std::vector<RunSlot *> free_slots;
   int active = 0;           // running jobs on this plan
   size_t bytes = 0;         // tables + the plan's own slot
@@ -190,6 +196,13 @@ int try_admit(beam_gpu_server *s, Job *j) {
     e->key = key;
     e->plan = p;
     e->bytes = info.device_bytes;
+    {
+      int least = 0, greatest = 0;  // e.g. 0 and -5: smaller numbers are served first
+      if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) least = greatest = 0;
+      int level = 0;
+      for (double t = (double)info.n_fourier_terms; t >= 1e9 && level < least - greatest; t /= 10.0) ++level;
+      e->priority = greatest + level;
+    }
     s->plans[key] = e;
     account(s, (long long)e->bytes);
     // a plan's size is known only once built: if it pushed the total over the
@@ -209,7 +222,7 @@ int try_admit(beam_gpu_server *s, Job *j) {
       finish(s, j, BEAM_JOB_FAILED, BEAM_EDEVMEM, "job footprint exceeds the server's memory budget");
       return BEAM_EDEVMEM;
     }
-    int rc = slot_create(p, 1, nullptr, &slot);
+    int rc = slot_create(p, 1, nullptr, &slot, e->priority);
     if (rc == BEAM_EDEVMEM && !s->active.empty()) return BEAM_EBUSY;
     if (rc != BEAM_OK) {
       finish(s, j, BEAM_JOB_FAILED, rc, beam_gpu_last_error_detail());

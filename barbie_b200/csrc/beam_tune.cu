@@ -145,7 +145,7 @@ extern "C" int beam_gpu_plan_autotune(beam_gpu_plan *p, int reps, beam_tune_repo
     if (cands[k].ms < cands[best].ms) best = k;
   // the kept decomposition, with fresh (zeroed) run buffers; after a failure
   // the default one
-  const int rc2 = rc == BEAM_OK ? rebuild(p, cands[best].tau0, cands[best].balance) : rebuild(p, TRI_TAU_MAX, 8.0);
+  const int rc2 = rc == BEAM_OK ? rebuild(p, cands[best].tau0, cands[best].balance) : rebuild(p, p->cfg.precision == BEAM_PREC_FP64 ? 2 * TRI_TAU_MAX : TRI_TAU_MAX, 8.0);
   if (rc == BEAM_OK) rc = rc2;
   if (rep && rc == BEAM_OK) {
     rep->n = (int)cands.size();
