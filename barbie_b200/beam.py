@@ -24,7 +24,7 @@ LIB_PATH = os.path.join(HERE, "libbeam_gpu.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "beam_gpu.h")
 
 NPOLES = 16
-PREC = {"fp64": 0, "mixed": 1}
+PREC = {"fp64": 0, "mixed": 1, "int8": 2}
 METHOD = {"triangle": 0, "pixel": 1}
 
 BEAM_OK = 0

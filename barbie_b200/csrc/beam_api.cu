@@ -119,7 +119,7 @@ void beam_gpu_destroy(beam_gpu_ctx *ctx) {
 int beam_gpu_plan_create(beam_gpu_ctx *ctx, const beam_cfg *cfg, beam_gpu_plan **out) {
   if (!ctx || !cfg || !out) return BEAM_EINVAL;
   *out = nullptr;
-  if ((cfg->precision != BEAM_PREC_FP64 && cfg->precision != BEAM_PREC_MIXED) ||
+  if ((cfg->precision != BEAM_PREC_FP64 && cfg->precision != BEAM_PREC_MIXED && cfg->precision != BEAM_PREC_INT8) ||
       (cfg->method != BEAM_METHOD_TRIANGLE && cfg->method != BEAM_METHOD_PIXEL)) {
     set_detail("unknown precision or method");
     return BEAM_EINVAL;
@@ -179,6 +179,10 @@ void beam_gpu_plan_destroy(beam_gpu_plan *p) {
 
 int beam_gpu_plan_set_triangle_launch(beam_gpu_plan *p, int mode) {
   if (!p || (mode != BEAM_LAUNCH_CLASSES && mode != BEAM_LAUNCH_PERSISTENT)) return BEAM_EINVAL;
+  if (p->cfg.precision == BEAM_PREC_INT8 && mode == BEAM_LAUNCH_PERSISTENT) {
+    set_detail("the int8 path has class launches only");
+    return BEAM_EINVAL;
+  }
   if (p->tri_launch == mode) return BEAM_OK;
   BEAM_CUDA(cudaSetDevice(p->ctx->device));
   BEAM_CUDA(cudaStreamSynchronize(p->ctx->stream));

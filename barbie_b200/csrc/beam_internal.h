@@ -86,6 +86,7 @@ enum : int { DEV_OK = 0, DEV_TIMEOUT = 1, DEV_BAD_INDEX = 2 };
 // pieces (a run's part within one chunk), one pipeline stage each, a run
 // longer than a chunk's room going on in the next chunk.
 constexpr int TRI_WARPS = 7;   // most tiles per CTA (one consumer warp each, plus one producer warp)
+constexpr int TRI_CLASSES = 12;  // most tiles per CTA on any path (int8: I8_MAX_TILES)
 constexpr int TRI_P1 = 8;      // planes p1 per thread
 constexpr int TRI_CHUNK = 16;  // in-plane triangles per stage
 constexpr int TRI_PIECES = 4;  // pieces per stage
@@ -155,7 +156,65 @@ struct TriItem {
   int tile0, ntiles;
   int m1, m2, m3;  // first mode of rings r1, r2, r3 in the mode table
   int colx, Lx, colz, Lz, coly, Ly;
+  int rx, rz;      // rings of the x leg (r1) and the tile leg (r3): their slice scales (int8 path)
 };
+
+// The int8 path (BEAM_PREC_INT8). Every mode value v of ring r on the plane of
+// column c is cut into five 8-bit slices against the scale 2^e(r, c) >
+// max |Re|, |Im| over the ring's modes there:
+//   v = 2^(e - 7) (a0 + a1 2^-8 + a2 2^-16 + a3 2^-24 + a4 2^-32 + d), 0 <= d < 2^-32,
+// a0 = floor(v 2^(7-e)) in [-128, 127] (signed), a1..a4 in [0, 255] (unsigned).
+// A run's outer product W(p1, p3) = sum x(p1) z(p3) is then
+//   2^(ex + ez - 14) sum_L 2^(-8L) acc_L,  acc_L = sum over slice pairs i + j = L < I8_LEVELS,
+// each acc_L an exact int32 sum of 8-bit products on the tensor cores. A
+// warp's tile is one window of I8_BW planes p3 (the MMA's 16 rows, z leg) x
+// up to two blocks of 8 planes p1 (its 8 columns each, x leg); a CTA's group
+// is I8_GROUP_WINDOWS windows x up to TRI_WARPS p1 blocks (at most
+// I8_MAX_TILES tiles); a chunk is 16
+// triangles of one run (the MMA's K = 32: 16 triangles x real, imaginary).
+// Slice rows: per mode, the x table (I8_XW words per column: slice s as the
+// bytes (Re, -Im, Im, Re)) and the z table (I8_ZW words per column: slices
+// (0,1), (2,3), (4) as (Re, Im) byte pairs), each column-interleaved so a
+// row segment is one copy.
+#ifndef BEAM_I8_NBT
+#define BEAM_I8_NBT 2
+#endif
+#ifndef BEAM_I8_MAX_TILES
+#define BEAM_I8_MAX_TILES 5
+#endif
+#ifndef BEAM_I8_STAGES
+#define BEAM_I8_STAGES 3
+#endif
+#ifndef BEAM_I8_MINB
+#define BEAM_I8_MINB 2
+#endif
+constexpr int I8_BW = 16;        // planes p3 per tile window
+constexpr int I8_NBT = BEAM_I8_NBT;              // p1 blocks per tile
+constexpr int I8_MAX_TILES = BEAM_I8_MAX_TILES;  // tiles per CTA (2 CTAs of 6 warps per SM at 168 registers)
+#ifndef BEAM_I8_GROUP_WINDOWS
+#define BEAM_I8_GROUP_WINDOWS 2
+#endif
+constexpr int I8_GROUP_WINDOWS = BEAM_I8_GROUP_WINDOWS;  // windows of a CTA's group
+constexpr int I8_STAGES = BEAM_I8_STAGES;        // pipeline depth
+constexpr int I8_MINB = BEAM_I8_MINB;            // CTAs per SM the register budget is sized for
+constexpr int I8_SLICES = 5;
+#ifndef BEAM_I8_LEVELS
+#define BEAM_I8_LEVELS 6
+#endif
+constexpr int I8_LEVELS = BEAM_I8_LEVELS;  // slice pairs i + j < I8_LEVELS are summed (6: the 19 pairs up to i + j = 5)
+constexpr int I8_XW = 5;         // x table words per column
+constexpr int I8_ZW = 3;         // z table words per column
+constexpr int I8_RUN_MAX = 2048; // longest run summed in int32 (|acc| < 2048 x 2 x 5 x 255^2 < 2^31)
+
+// int8 path staging. A chunk's stage holds, per triangle, the x leg's table
+// segment (Lx columns x I8_XW words) and the z leg's (Lz x I8_ZW), then the
+// run leg's FP64 row (Ly columns). Triangle rows are i8_pitch(words) apart:
+// rounded up to 4 (mod 8), so the 32 lanes' words (column g, triangle rows 2t)
+// fall on 32 distinct banks for both 5- and 3-word columns.
+__host__ __device__ inline int i8_pitch(int words) { return words + ((12 - (words & 7)) & 7); }
+__host__ __device__ inline int i8_stage_bytes(const TriItem &it) {
+  return TRI_CHUNK * (i8_pitch(I8_XW * it.Lx) + i8_pitch(I8_ZW * it.Lz)) * 4 + it.Ly * 16;
+}
 
 // Device-side tables of a plan (read-only while it runs; per-run buffers live
 // in RunSlot).
@@ -191,10 +250,13 @@ struct DevPlan {
   int n_items = 0;
   TriItem *items = nullptr;       // [n_items]: grouped by tile count, largest work first in a group
   int32_t *q_order = nullptr;     // [n_items] items in decreasing order of work (persistent kernel)
-  int class_first[TRI_WARPS + 2] = {};  // items with n tiles: [class_first[n], class_first[n+1])
-  int class_stage[TRI_WARPS + 1] = {};  // stage size (complex values) of the CTAs with n tiles
+  int class_first[TRI_CLASSES + 2] = {};  // items with n tiles: [class_first[n], class_first[n+1])
+  int class_stage[TRI_CLASSES + 1] = {};  // stage size (complex values; int8: bytes) of the CTAs with n tiles
   long long n_part = 0;           // partial-sum slots per realization
-  size_t elem = 0;                // bytes of one complex mode value (16 FP64, 8 mixed)
+  size_t elem = 0;                // bytes of one complex mode value (16 FP64, 8 mixed, 48 int8: FP64 + slices)
+  int i8 = 0;                     // int8 path: S holds FP64 rows, slice rows, then ring scales
+  int n_rings = 0;
+  int32_t *ring_first = nullptr;  // [n_rings + 1] first mode of each ring (int8 path)
   // epilogue (bin order)
   int n_bins = 0;
   int32_t *bin_first = nullptr;   // [n_bins+1]
@@ -206,6 +268,17 @@ struct DevPlan {
   int32_t *bin_chunk = nullptr;   // [n_bins+1] chunk ranges per bin
 };
 constexpr int EP_CHUNK = 1024;  // most triangles per epilogue CTA
+
+// Bytes of one realization's mode data. The int8 path keeps, after the FP64
+// rows (the run leg's values), the x and z slice tables (I8_XW and I8_ZW
+// words per mode and column) and the scale exponents e(r, c) (int32 [n_rings][W]).
+inline size_t i8_fp64_bytes(const DevPlan &d) { return (size_t)d.n_modes * d.W * 16; }
+inline size_t i8_xtab_bytes(const DevPlan &d) { return (size_t)d.n_modes * d.W * I8_XW * 4; }
+inline size_t i8_slice_bytes(const DevPlan &d) { return (size_t)d.n_modes * d.W * (I8_XW + I8_ZW) * 4; }
+inline size_t mode_data_bytes(const DevPlan &d) {
+  if (!d.i8) return d.elem * (size_t)d.n_modes * d.W;
+  return i8_fp64_bytes(d) + i8_slice_bytes(d) + (((size_t)d.n_rings * d.W * 4 + 255) & ~(size_t)255);
+}
 // sections of a realization's bin array: sum B*bs, sum Num*norm, bs/(vol*norm),
 // sum Biana*Num*bs (each [n_bins][16])
 constexpr int BIN_SECTIONS = 4;
@@ -213,8 +286,8 @@ constexpr int BIN_SECTIONS = 4;
 // A stream plus the side streams the per-class triangle-sum launches fork onto.
 struct Lane {
   cudaStream_t stream = nullptr;
-  cudaStream_t side[TRI_WARPS] = {};
-  cudaEvent_t fork = nullptr, join[TRI_WARPS] = {};
+  cudaStream_t side[TRI_CLASSES] = {};
+  cudaEvent_t fork = nullptr, join[TRI_CLASSES] = {};
 };
 // priority: the streams' CUDA priority (0 = default; lower is more urgent)
 int lane_create(Lane *l, int priority = 0);
@@ -327,6 +400,9 @@ void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c, i
 int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged, bool staged_on_device = false);
 int gather_mapped(beam_gpu_plan *p, RunSlot *s, const double *r2c_mapped);
 int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n);
+// int8 path (beam_tri_i8.cu)
+int launch_triangle_i8(beam_gpu_plan *p, RunSlot *s, int nreal);
+int triangle_i8_init_attributes(size_t smem_optin);
 int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n);
 int fetch_results(beam_gpu_plan *p, RunSlot *s, int n);
 int check_status(RunSlot *s);

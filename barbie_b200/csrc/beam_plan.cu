@@ -376,6 +376,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     int tile0, ntiles;
     int p1lo, p1hi, p3lo, p3hi, p2lo, p2hi;  // over accepted combos
     int tp1lo, tp1hi;                        // first plane p1 of the tiles
+    int w3lo, w3hi;                          // int8: first plane p3 of the group's first and last window
   };
   std::vector<TriTile> tiles;
   std::vector<int32_t> tile_combo;
@@ -392,6 +393,12 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   // non-empty blocks is kept: fewer MMA cells without a combo. Triplets are
   // searched in parallel; each block is marked with the number of the origin
   // being counted, so the marks need no clearing between origins.
+  // Block geometry: TRI_P1 planes p1 x BW planes p3, NBT blocks per tile. The
+  // int8 path's tile is one window of I8_BW planes p3 x up to two p1 blocks
+  // (a group is one window); the others pack any four 8 x 8 blocks of a
+  // 32-plane p3 window.
+  const bool i8 = p->cfg.precision == BEAM_PREC_INT8;
+  const int BW = i8 ? I8_BW : TRI_BW, NBT = i8 ? I8_NBT : TRI_BLOCKS;
   struct Origin {
     int p3min, o1, o3;
   };
@@ -406,18 +413,19 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
         p1max = std::max(p1max, combo_p1[c]);
       }
       Origin o{p3min, 0, 0};
-      const int nb1 = (p1max + 4) / TRI_P1 + 1, nb3 = (p3max - p3min + TRI_BW - 1) / TRI_BW + 1;
+      const int nb1 = (p1max + 4) / TRI_P1 + 1, nb3 = (p3max - p3min + BW - 1) / BW + 1;
       std::vector<uint8_t> mark((size_t)nb1 * nb3, 0);
       int best = 1 << 30;
       uint8_t stamp = 0;
-      const int a3first = (A == 4) ? ((p3min % 4) + 4) % 4 : 0, a3step = (A == 4) ? 4 : 1;
+      const bool f4 = (A == 4) && !i8;  // the mixed consumer's aligned float4 reads
+      const int a3first = f4 ? ((p3min % 4) + 4) % 4 : 0, a3step = f4 ? 4 : 1;
       for (int a1 = 0; a1 < TRI_P1; a1 += 4)
-        for (int a3 = a3first; a3 < TRI_BW; a3 += a3step) {
+        for (int a3 = a3first; a3 < BW; a3 += a3step) {
           ++stamp;
           int nblocks = 0;
           for (int c = cf; c < cf + nc; ++c) {
             const int p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
-            uint8_t &m = mark[(size_t)((p1 + a1) / TRI_P1) * nb3 + (p3 - p3min + a3) / TRI_BW];
+            uint8_t &m = mark[(size_t)((p1 + a1) / TRI_P1) * nb3 + (p3 - p3min + a3) / BW];
             nblocks += (m != stamp);
             m = stamp;
           }
@@ -445,33 +453,43 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     std::vector<Slot> slots(nc);
     for (int k = 0; k < nc; ++k) {
       int c = cf + k, p1 = combo_p1[c], p3 = -p1 - combo_p2[c];
-      long long bp1 = (p1 + o1) / TRI_P1, b3 = (p3 - p3min + o3) / TRI_BW;
+      long long bp1 = (p1 + o1) / TRI_P1, b3 = (p3 - p3min + o3) / BW;
       // a group is one window of 32 planes p3 over up to TRI_WARPS blocks of
-      // planes p1; its non-empty TRI_P1 x TRI_BW blocks are packed four to a tile
-      slots[k] = Slot{(b3 / TRI_BLOCKS) * 1000000 + bp1 / TRI_WARPS, bp1 * 1000000 + b3, (p1 + o1) % TRI_P1,
-                      (p3 - p3min + o3) % TRI_BW, c};
+      // planes p1; its non-empty TRI_P1 x TRI_BW blocks are packed four to a
+      // tile (int8: one I8_BW window over up to 2 TRI_WARPS p1 blocks, two to a tile)
+      // (int8: I8_GROUP_WINDOWS windows over up to TRI_WARPS p1 blocks, a tile being two p1
+      // blocks of one window, the blocks window-major)
+      const long long gkey =
+          i8 ? (b3 / I8_GROUP_WINDOWS) * 1000000 + bp1 / TRI_WARPS : (b3 / TRI_BLOCKS) * 1000000 + bp1 / TRI_WARPS;
+      const long long tkey = i8 ? b3 * 1000000 + bp1 : bp1 * 1000000 + b3;
+      slots[k] = Slot{gkey, tkey, (p1 + o1) % TRI_P1, (p3 - p3min + o3) % BW, c};
     }
     std::sort(slots.begin(), slots.end(), [](const Slot &x, const Slot &y) {
       return x.gkey != y.gkey ? x.gkey < y.gkey : (x.tkey != y.tkey ? x.tkey < y.tkey : x.c < y.c);
     });
     for (size_t k = 0; k < slots.size();) {
       Group gr{(int)tiles.size(), 0, 1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30),
-               1 << 30, -(1 << 30)};
+               1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
       long long gk = slots[k].gkey;
-      while (k < slots.size() && slots[k].gkey == gk) {
+      while (k < slots.size() && slots[k].gkey == gk && (!i8 || gr.ntiles < I8_MAX_TILES)) {
         TriTile tl;
         tiles.push_back(tl);
         tile_combo.resize(tiles.size() * TRI_P1 * 32, -1);
         int32_t *tc = tile_combo.data() + (tiles.size() - 1) * TRI_P1 * 32;
         int nb = 0;
-        for (; nb < TRI_BLOCKS && k < slots.size() && slots[k].gkey == gk; ++nb) {
+        for (; nb < NBT && k < slots.size() && slots[k].gkey == gk &&
+               (!i8 || nb == 0 || slots[k].tkey / 1000000 == slots[k - 1].tkey / 1000000);
+             ++nb) {
           long long bk = slots[k].tkey;
           int bp1 = (int)(bk / 1000000), b3 = (int)(bk % 1000000);
+          if (i8) std::swap(bp1, b3);
           tl.p1_0[nb] = bp1 * TRI_P1 - o1;
-          tl.p3_0[nb] = p3min - o3 + b3 * TRI_BW;
+          tl.p3_0[nb] = p3min - o3 + b3 * BW;
+          gr.w3lo = std::min(gr.w3lo, tl.p3_0[nb]);
+          gr.w3hi = std::max(gr.w3hi, tl.p3_0[nb]);
           for (; k < slots.size() && slots[k].tkey == bk && slots[k].gkey == gk; ++k) {
             const Slot &s = slots[k];
-            tc[s.a * 32 + nb * TRI_BW + s.lane] = s.c;
+            tc[s.a * 32 + nb * BW + s.lane] = s.c;
             int p1 = combo_p1[s.c], p2 = combo_p2[s.c], p3 = -p1 - p2;
             gr.p1lo = std::min(gr.p1lo, p1); gr.p1hi = std::max(gr.p1hi, p1);
             gr.p2lo = std::min(gr.p2lo, p2); gr.p2hi = std::max(gr.p2hi, p2);
@@ -488,7 +506,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
         tiles.back() = tl;
         gr.ntiles++;
       }
-      if (gr.ntiles > TRI_WARPS) too_big[u] = 1;
+      if (gr.ntiles > (i8 ? I8_MAX_TILES : TRI_WARPS)) too_big[u] = 1;
       groups[u].push_back(gr);
     }
   };
@@ -561,7 +579,11 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
     const long long nt = p->tri_first[u + 1] - p->tri_first[u];
     std::vector<int2> runs;  // (length, k2)
     for (long long k = k2base[u]; k < k2base[u + 1]; ++k)
-      if (k2cnt[k] > 0) runs.push_back(make_int2(k2cnt[k], (int)(k - k2base[u])));
+      for (int left = k2cnt[k]; left > 0;) {  // int8: runs of at most I8_RUN_MAX (exact int32 sums)
+        const int len = i8 ? std::min(left, I8_RUN_MAX) : left;
+        runs.push_back(make_int2(len, (int)(k - k2base[u])));
+        left -= len;
+      }
     int ns = splits(u, tau_max);
     u_nsplit[u] = ns;
     u_part[u + 1] = u_part[u] + (long long)ns * u_ncombo[u];
@@ -593,7 +615,8 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
         int left = runs[r].x;
         bool cont = false;
         while (left > 0) {
-          if (cnpc == TRI_PIECES || TRI_CHUNK - cnt_ < std::min(left, 4)) close_chunk();
+          // int8: one run per chunk (a chunk is one MMA depth of 16 triangles)
+          if (cnpc == TRI_PIECES || TRI_CHUNK - cnt_ < std::min(left, 4) || (i8 && cnt_ > 0)) close_chunk();
           const int room = TRI_CHUNK - cnt_;  // >= 4 whenever the run does not fit
           const int len = left <= room ? left : (room / 4) * 4;
           const bool more = len < left;
@@ -632,6 +655,12 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
         const int cb = d.colbase, ext = TRI_P1 - 1;
         it.colx = floorA(gr.tp1lo + cb); it.Lx = ceilA(gr.tp1hi + ext + cb + 1) - it.colx;
         it.colz = floorA(gr.p3lo + cb); it.Lz = ceilA(gr.p3hi + cb + 1) - it.colz;
+        if (i8) {  // the group's windows (rows outside the mode rows read column 0)
+          it.colz = std::max(0, floorA(gr.w3lo + cb));
+          it.Lz = std::min(d.W, ceilA(gr.w3hi + I8_BW + cb)) - it.colz;
+        }
+        it.rx = g.rp[3 * rp];
+        it.rz = g.rp[3 * rp + lz];
         it.coly = floorA(gr.p2lo - ext + cb); it.Ly = ceilA(gr.p2hi + ext + cb + 1) - it.coly;
         if (it.colx < 0 || it.colx + it.Lx > d.W || it.colz < 0 || it.colz + it.Lz > d.W || it.coly < 0 ||
             it.coly + it.Ly > d.W)
@@ -653,7 +682,7 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
       }
       for (int c = u_cfirst[u]; c < u_cfirst[u] + u_ncombo[u]; ++c) seen[c] = 2;
     }
-    if (A == 4)  // the mixed consumer's float4 reads of x and z
+    if (A == 4 && !i8)  // the mixed consumer's float4 reads of x and z
       for (const TriTile &tl : tiles)
         for (int n = 0; n < TRI_BLOCKS; ++n)
           if ((tl.p1_0[n] & 3) || (tl.p3_0[n] & 3)) return set_detail("mixed tile block off a 4-plane boundary"), BEAM_EINVAL;
@@ -704,17 +733,20 @@ static int build_work(beam_gpu_plan *p, const std::vector<int32_t> &u_cfirst, co
   std::stable_sort(q_order.begin(), q_order.end(), [&](int x, int y) { return work[order[x]] > work[order[y]]; });
   size_t elem = (A == 1) ? 16 : 8;
   size_t budget = p->ctx->smem_optin > 4096 ? p->ctx->smem_optin - 4096 : 48 * 1024;
-  for (int n = 0; n <= TRI_WARPS + 1; ++n) d.class_first[n] = 0;
-  for (int n = 0; n <= TRI_WARPS; ++n) d.class_stage[n] = 0;
+  for (int n = 0; n <= TRI_CLASSES + 1; ++n) d.class_first[n] = 0;
+  for (int n = 0; n <= TRI_CLASSES; ++n) d.class_stage[n] = 0;
   for (const TriItem &it : sorted) {
     d.class_first[it.ntiles + 1]++;
     const bool f64 = (A == 1);
     int stage = TRI_CHUNK * (stage_pitch(it.Lx, f64) + stage_pitch(it.Lz, f64)) + TRI_PIECES * it.Ly;
+    if (i8) stage = i8_stage_bytes(it);  // in bytes
     d.class_stage[it.ntiles] = std::max(d.class_stage[it.ntiles], stage);
   }
-  for (int n = 0; n <= TRI_WARPS; ++n) d.class_first[n + 1] += d.class_first[n];
-  for (int n = 1; n <= TRI_WARPS; ++n)
-    if ((size_t)TRI_STAGES * d.class_stage[n] * elem > budget) {
+  if (i8) elem = 1;
+  for (int n = 0; n <= TRI_CLASSES; ++n) d.class_first[n + 1] += d.class_first[n];
+  for (int n = 1; n <= TRI_CLASSES; ++n)
+    if ((size_t)(i8 ? I8_STAGES : TRI_STAGES) * d.class_stage[n] * elem + (i8 ? (size_t)n * 8 * 32 * sizeof(double) : 0) >
+        budget) {
       set_detail("staged mode rows do not fit shared memory");
       return BEAM_EINVAL;
     }
@@ -771,8 +803,10 @@ int build_plan_tables(beam_gpu_plan *p) {
   // bulk copies move whole 16-byte units: rows, their starts and lengths are
   // kept in multiples of A complex values (1 for complex128; 4 for the mixed
   // path, whose rows hold blocks of 4 real parts then their 4 imaginary parts,
-  // so a copied segment starts and ends on a whole block)
-  const int A = (p->cfg.precision == BEAM_PREC_MIXED) ? 4 : 1;
+  // so a copied segment starts and ends on a whole block; 4 for the int8
+  // path, whose slice sub-rows hold 4 bytes per column)
+  const bool i8 = p->cfg.precision == BEAM_PREC_INT8;
+  const int A = (p->cfg.precision == BEAM_PREC_MIXED || i8) ? 4 : 1;
   auto floorA = [A](int v) { return v - (((v % A) + A) % A); };
   auto ceilA = [A, &floorA](int v) { return floorA(v + A - 1); };
   d.Q = Q;
@@ -943,7 +977,10 @@ int build_plan_tables(beam_gpu_plan *p) {
   BEAM_TRY(upload(p, &d.ep_ana, ep_ana));
   BEAM_TRY(upload(p, &d.ep_cnt, ep_cnt));
 
-  d.elem = (p->cfg.precision == BEAM_PREC_MIXED) ? sizeof(float2) : sizeof(double2);
+  d.elem = (p->cfg.precision == BEAM_PREC_MIXED) ? sizeof(float2) : (i8 ? 48 : sizeof(double2));
+  d.i8 = i8 ? 1 : 0;
+  d.n_rings = (int)Nr;
+  if (i8) BEAM_TRY(upload(p, &d.ring_first, p->ring_first));
   p->build_ms[3] = ms(t2, now());
   return BEAM_OK;
 }
@@ -953,7 +990,7 @@ void free_plan_tables(beam_gpu_plan *p) {
   void *ptrs[] = {d.mode_ij,  d.mode_neg, d.ringmap, d.pixlocal,   d.tri_list, d.combo_u, d.combo_out,
                   d.u_cfirst, d.u_ncombo, d.u_nsplit, d.u_part,    d.tiles,    d.tile_combo, d.chunks,
                   d.pieces,   d.descs,    d.items,    d.q_order,   d.bin_first, d.ep_px,  d.ep_pz,   d.ep_cnt,
-                  d.ep_chunk_first, d.bin_chunk, d.ep_ana};
+                  d.ep_chunk_first, d.bin_chunk, d.ep_ana, d.ring_first};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   d = DevPlan();

@@ -37,14 +37,15 @@ struct CplxOf<float2> {
 // blocked by 4 columns (mixed_re: 4 real parts, then their 4 imaginary
 // parts), so its consumer loads 4 planes' real or imaginary parts at once
 // and multiplies pairs of planes with packed FP32 FMAs.
+// real_stride: elements of C from one realization's rows to the next's.
 template <typename C>
 __global__ void k_build_modes(const double *const *__restrict__ srcs, int staged, const int16_t *__restrict__ mode_ij,
                               const int32_t *__restrict__ mode_neg, int n_modes, int Q, int W, int colbase, int NN,
-                              C *__restrict__ S) {
+                              C *__restrict__ S, long long real_stride) {
   long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long long)n_modes * W) return;
   const double2 *src = reinterpret_cast<const double2 *>(srcs[blockIdx.y]);
-  S += (size_t)blockIdx.y * n_modes * W;
+  S += (size_t)blockIdx.y * real_stride;
   int m = (int)(idx / W), w = (int)(idx % W);
   int q = w - colbase;
   C v = CplxOf<C>::make(0.0, 0.0);
@@ -65,6 +66,110 @@ __global__ void k_build_modes(const double *const *__restrict__ srcs, int staged
   } else {
     S[idx] = v;
   }
+}
+
+// ------------------------------------------------------- int8 slice rows
+// Scale exponent e(r, c) of ring r on the plane of column c: the smallest e
+// with max |Re|, |Im| over the ring's modes there below 2^e (0 for a column
+// of zeros). CTA: 32 columns x 8 strides over the ring's modes, one ring
+// (blockIdx.x / ceil(W / 32)); realization blockIdx.y.
+__global__ void k_ring_scale(const double2 *__restrict__ S, long long real_stride, const int32_t *__restrict__ ring_first,
+                             int W, int32_t *__restrict__ scale, long long scale_stride) {
+  __shared__ double s_max[8][32];
+  const int cblocks = (W + 31) / 32;
+  const int r = blockIdx.x / cblocks, c = (blockIdx.x % cblocks) * 32 + (threadIdx.x & 31), k = threadIdx.x >> 5;
+  S += (size_t)blockIdx.y * real_stride;
+  double mx = 0.0;
+  if (c < W)
+    for (int m = ring_first[r] + k; m < ring_first[r + 1]; m += 8) {
+      const double2 v = S[(size_t)m * W + c];
+      mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+  s_max[k][threadIdx.x & 31] = mx;
+  __syncthreads();
+  if (k == 0 && c < W) {
+    for (int j = 1; j < 8; ++j) mx = fmax(mx, s_max[j][threadIdx.x]);
+    int e = 0;
+    if (mx > 0.0) frexp(mx, &e);  // mx = f 2^e with f in [0.5, 1)
+    scale[(size_t)blockIdx.y * scale_stride + (size_t)r * W + c] = e;
+  }
+}
+
+// The five slices of v against 2^e (|v| < 2^e): a0 = floor(v 2^(7-e)) in
+// [-128, 127], then a1..a4 = the next four base-256 digits of the remainder
+// in [0, 1), each step exact in FP64. Byte k of the result's low and high
+// words is slice k (slices 0-3 in lo, 4 in hi).
+__device__ __forceinline__ void slice5(double v, int e, uint32_t &lo, uint32_t &hi) {
+  double u = ldexp(v, 7 - e);
+  double a = floor(u);
+  double rem = u - a;
+  lo = (uint32_t)((int)a & 0xff);
+  hi = 0;
+#pragma unroll
+  for (int k = 1; k < I8_SLICES; ++k) {
+    rem *= 256.0;
+    a = floor(rem);
+    rem -= a;
+    if (k < 4) lo |= (uint32_t)a << (8 * k);
+    else hi = (uint32_t)a;
+  }
+}
+
+// Slice tables of every mode (realization blockIdx.y). The x table holds per
+// (mode, column) I8_XW words: word s = slice s of (Re, -Im, Im, Re) as bytes
+// 0-3 (the x leg's two operand orders); the z table I8_ZW words: (Re, Im)
+// pairs of slices (0, 1), (2, 3) and (4) (the z leg's operand). The slices of
+// -Im are those of the negated value, not negated slices (slices 1-4 are
+// unsigned).
+__global__ void k_build_slices(const double2 *__restrict__ S, long long real_stride, const int32_t *__restrict__ ring_first,
+                               int n_rings, int n_modes, int W, const int32_t *__restrict__ scale, long long scale_stride,
+                               uint32_t *__restrict__ xtab, uint32_t *__restrict__ ztab, long long tab_stride) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n_modes * W) return;
+  const int m = (int)(idx / W), c = (int)(idx % W);
+  int lo = 0, hi = n_rings;  // ring of mode m: ring_first[r] <= m < ring_first[r + 1]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (ring_first[mid] <= m) lo = mid; else hi = mid;
+  }
+  const double2 v = S[(size_t)blockIdx.y * real_stride + idx];
+  const int e = scale[(size_t)blockIdx.y * scale_stride + (size_t)lo * W + c];
+  uint32_t re0, re4, im0, im4, ni0, ni4;
+  slice5(v.x, e, re0, re4);
+  slice5(v.y, e, im0, im4);
+  slice5(-v.y, e, ni0, ni4);
+  uint32_t *xo = xtab + (size_t)blockIdx.y * tab_stride + (size_t)idx * I8_XW;
+#pragma unroll
+  for (int k = 0; k < I8_XW; ++k) {
+    const uint32_t r = k < 4 ? (re0 >> (8 * k)) & 0xff : re4, i = k < 4 ? (im0 >> (8 * k)) & 0xff : im4,
+                   n = k < 4 ? (ni0 >> (8 * k)) & 0xff : ni4;
+    xo[k] = r | (n << 8) | (i << 16) | (r << 24);
+  }
+  uint32_t *zo = ztab + (size_t)blockIdx.y * tab_stride + (size_t)idx * I8_ZW;
+  zo[0] = (re0 & 0xff) | ((im0 & 0xff) << 8) | (((re0 >> 8) & 0xff) << 16) | (((im0 >> 8) & 0xff) << 24);
+  zo[1] = ((re0 >> 16) & 0xff) | (((im0 >> 16) & 0xff) << 8) | ((re0 >> 24) << 16) | ((im0 >> 24) << 24);
+  zo[2] = re4 | (im4 << 8);
+}
+
+// Scales and slice rows of realizations [0, n) from their FP64 rows.
+static int build_slices(beam_gpu_plan *p, RunSlot *s, int n) {
+  const DevPlan &d = p->d;
+  cudaStream_t st = s->lane->stream;
+  const long long real_bytes = (long long)mode_data_bytes(d);
+  const double2 *S = (const double2 *)s->S;
+  uint32_t *xtab = (uint32_t *)((unsigned char *)s->S + i8_fp64_bytes(d));
+  uint32_t *ztab = (uint32_t *)((unsigned char *)s->S + i8_fp64_bytes(d) + i8_xtab_bytes(d));
+  int32_t *scale = (int32_t *)((unsigned char *)s->S + i8_fp64_bytes(d) + i8_slice_bytes(d));
+  const int cblocks = (d.W + 31) / 32;
+  k_ring_scale<<<dim3((unsigned)(d.n_rings * cblocks), (unsigned)n), 256, 0, st>>>(
+      S, real_bytes / 16, d.ring_first, d.W, scale, real_bytes / 4);
+  BEAM_CUDA(cudaGetLastError());
+  const long long per = (long long)d.n_modes * d.W;
+  k_build_slices<<<dim3((unsigned)((per + 255) / 256), (unsigned)n), 256, 0, st>>>(
+      S, real_bytes / 16, d.ring_first, d.n_rings, d.n_modes, d.W, scale, real_bytes / 4, xtab, ztab, real_bytes / 4);
+  BEAM_CUDA(cudaGetLastError());
+  s->launches += 2;
+  return BEAM_OK;
 }
 
 // ----------------------------------------------------------------- epilogue
@@ -206,7 +311,7 @@ __global__ void k_ep_bins(const int32_t *__restrict__ bin_chunk, int n_bins, int
 // ------------------------------------------------------------ host drivers
 int lane_create(Lane *l, int priority) {
   cudaError_t e = cudaStreamCreateWithPriority(&l->stream, cudaStreamNonBlocking, priority);
-  for (int k = 0; k < TRI_WARPS && e == cudaSuccess; ++k) {
+  for (int k = 0; k < TRI_CLASSES && e == cudaSuccess; ++k) {
     e = cudaStreamCreateWithPriority(&l->side[k], cudaStreamNonBlocking, priority);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&l->join[k], cudaEventDisableTiming);
   }
@@ -220,7 +325,7 @@ int lane_create(Lane *l, int priority) {
 }
 
 void lane_destroy(Lane *l) {
-  for (int k = 0; k < TRI_WARPS; ++k) {
+  for (int k = 0; k < TRI_CLASSES; ++k) {
     if (l->side[k]) cudaStreamDestroy(l->side[k]);
     if (l->join[k]) cudaEventDestroy(l->join[k]);
   }
@@ -239,7 +344,7 @@ static SlotSizes slot_sizes(const beam_gpu_plan *p, int cap) {
   SlotSizes z;
   z.staging = sizeof(double) * 2 * c * (size_t)d.n_modes * d.Q;
   z.src = sizeof(double *) * 2 * c;
-  z.S = d.elem * c * (size_t)d.n_modes * d.W;
+  z.S = c * mode_data_bytes(d);
   z.part = sizeof(double) * c * (size_t)d.n_part;
   z.B = sizeof(double) * c * (size_t)std::max<long long>(1, d.n_combo);
   z.bins = sizeof(double) * c * BIN_SECTIONS * (size_t)d.n_bins * BEAM_NPOLES;
@@ -383,14 +488,16 @@ int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged, bool staged_o
   if (per == 0) return BEAM_OK;
   dim3 grid((unsigned)((per + 255) / 256), (unsigned)n);
   const double *const *srcs = staged ? s->src : s->src + s->cap;
-  if (d.elem == sizeof(double2))
-    k_build_modes<double2><<<grid, 256, 0, st>>>(srcs, staged ? 1 : 0, d.mode_ij, d.mode_neg, d.n_modes, d.Q, d.W,
-                                                 d.colbase, (int)p->geom.NN, (double2 *)s->S);
-  else
+  if (d.elem == sizeof(float2))
     k_build_modes<float2><<<grid, 256, 0, st>>>(srcs, staged ? 1 : 0, d.mode_ij, d.mode_neg, d.n_modes, d.Q, d.W,
-                                                d.colbase, (int)p->geom.NN, (float2 *)s->S);
+                                                d.colbase, (int)p->geom.NN, (float2 *)s->S, per);
+  else
+    k_build_modes<double2><<<grid, 256, 0, st>>>(srcs, staged ? 1 : 0, d.mode_ij, d.mode_neg, d.n_modes, d.Q, d.W,
+                                                 d.colbase, (int)p->geom.NN, (double2 *)s->S,
+                                                 (long long)(mode_data_bytes(d) / sizeof(double2)));
   BEAM_CUDA(cudaGetLastError());
   s->launches++;
+  if (d.i8) BEAM_TRY(build_slices(p, s, n));
   return BEAM_OK;
 }
 

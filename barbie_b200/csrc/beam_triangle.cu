@@ -683,6 +683,7 @@ static int allow_optin(size_t smem_optin) {
 int triangle_init_attributes(size_t smem_optin) {
   BEAM_TRY(allow_optin<double2>(smem_optin));
   BEAM_TRY(allow_optin<float2>(smem_optin));
+  BEAM_TRY(triangle_i8_init_attributes(smem_optin));
   return BEAM_OK;
 }
 
@@ -775,7 +776,9 @@ int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n) {
   a.part_stride = d.n_part;
   mark(s, 1);
   const bool persistent = p->tri_launch == BEAM_LAUNCH_PERSISTENT;
-  if (d.elem == sizeof(double2))
+  if (d.i8)
+    BEAM_TRY(launch_triangle_i8(p, s, n));
+  else if (d.elem == sizeof(double2))
     BEAM_TRY(persistent ? launch_persistent<double2>(p, s, a) : launch_classes<double2>(p, s, a));
   else
     BEAM_TRY(persistent ? launch_persistent<float2>(p, s, a) : launch_classes<float2>(p, s, a));

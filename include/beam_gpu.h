@@ -57,6 +57,9 @@ extern "C" {
 /* precision of the triple-product sums */
 #define BEAM_PREC_FP64 0  /* FP64 throughout (parity path, 1e-10 of the reference) */
 #define BEAM_PREC_MIXED 1 /* FP32 mode data and products, FP32 chunk sums, FP64 across chunks */
+#define BEAM_PREC_INT8 2  /* FP64 mode data cut into five 8-bit slices per (ring, plane) scale; the
+                             slice products and each run's sums exact in int32 on the int8 tensor
+                             cores; FP64 from the run's end on (error ~1e-7 of a bin, far below 1e-5) */
 
 /* how the per-triangle sums B = sum_x Re(F1 F2 F3) are formed */
 #define BEAM_METHOD_TRIANGLE 0 /* over closed in-plane Fourier triangles (default) */
