@@ -351,6 +351,27 @@ def run_ours(args):
     else:
         oracle_ref = oracle_fixture_bins(fields[0]) if rank == 0 else None
 
+    # int8 path: exact slice products on the int8 tensor cores (errors per (l,m,bin) against FP64 and the oracle)
+    int8 = None
+    if not args.no_mixed:
+        plan_i = beam.Plan(ctx, W["NN"], W["UL_k1"], W["LL_k1"], W["BW_k1"], Nmax=W["Nmax"], Nr=W["Nr"],
+                           n_mtbin=W["n_mtbin"], precision="int8")
+        timed_loop(plan_i, dev_fields, args.warmup)
+        barrier()
+        it_, itri = timed_loop(plan_i, dev_fields, args.steps)
+        barrier()
+        i_total = max_over_ranks(sum(it_))
+        ref = plan.run(dev_fields[0])
+        got = plan_i.run(dev_fields[0])
+        int8 = {"value": world * args.steps / (i_total / 1e3) * 3600.0, "unit": UNIT,
+                "ms_per_step": i_total / args.steps, "triangle_kernel_ms": float(np.mean(itri)),
+                "speedup_vs_fp64": (sum(times) / sum(it_)), **mixed_errors(ref, got),
+                "launches_per_step": plan_i.refresh_info()["launches_last_run"]}
+        if oracle_ref is not None:
+            int8["vs_oracle"] = {k: v for k, v in mixed_errors(oracle_ref, got).items()
+                                 if k in ("max_rel_err", "median_rel_err", "frac_within_1e-5")}
+        plan_i.close()
+
     # FP64 bins against the oracle's bins of the same field (committed fixture)
     fp64_vs_oracle = None
     if oracle_ref is not None:
@@ -408,6 +429,9 @@ def run_ours(args):
         "mixed_max_rel_err": mixed["max_rel_err"] if mixed else None,
         "mixed_median_rel_err": mixed["median_rel_err"] if mixed else None,
         "mixed_roofline_frac": mixed["roofline"]["frac"] if mixed else None,
+        "int8_value": int8["value"] if int8 else None,
+        "int8_speedup": int8["speedup_vs_fp64"] if int8 else None,
+        "int8_max_rel_err": int8["max_rel_err"] if int8 else None,
         "serve_jobs": args.serve_jobs if serving else 0,
         "serve_p50_ms": serving["fp64"]["p50_ms"] if serving else None,
         "serve_p99_ms": serving["fp64"]["p99_ms"] if serving else None,
@@ -420,7 +444,7 @@ def run_ours(args):
         "cold_start_ms": cold["total_ms"],
         "latency_p50_ms": lat["p50_ms"], "latency_p99_ms": lat["p99_ms"],
     }
-    details = {"roofline": roofline, "mixed": mixed, "fp64_vs_oracle": fp64_vs_oracle, "cpu_baseline": cpu,
+    details = {"roofline": roofline, "mixed": mixed, "int8": int8, "fp64_vs_oracle": fp64_vs_oracle, "cpu_baseline": cpu,
                "cold_start": cold, "latency": lat, "persistent_launch": persistent, "wall_s": wall, "batched": batched, "serving": serving,
                "field": field, "autotune": tuning,
                "plan": {"n_triples": info["n_triples"], "n_fourier_terms": info["n_fourier_terms"],
