@@ -91,6 +91,7 @@ constexpr int TRI_P1 = 8;      // planes p1 per thread
 constexpr int TRI_CHUNK = 16;  // in-plane triangles per stage
 constexpr int TRI_PIECES = 4;  // pieces per stage
 constexpr int TRI_STAGES = 3;  // pipeline depth
+constexpr int TRI_META_AHEAD = 4;  // chunks whose descriptors the producer has in flight ahead of their copies
 constexpr int TRI_PAD = 8;     // zero columns on each side of a mode row (>= TRI_P1 - 1)
 
 // A warp's tile: TRI_BLOCKS blocks of TRI_P1 planes p1 x TRI_BW planes p3 of

@@ -178,8 +178,8 @@ __device__ __forceinline__ void i8_chunk(const uint32_t *xs, const uint32_t *zs,
 // each cell with a combo stores sum x 2^(ex(p1) + ez(p3) - 14).
 __device__ __forceinline__ void i8_consume(const I8Args &a, const TriItem &it, const unsigned char *S,
                                            const unsigned char *stages, uint64_t *full, uint64_t *empty,
-                                           volatile int *s_fail, int warp, int lane, int nch, int real,
-                                           double *sum) {
+                                           volatile int *s_fail, const volatile int *s_packed, int warp, int lane,
+                                           int nch, int real, double *sum) {
   const TriTile tl = a.tiles[it.tile0 + warp];
   const int nblk = tl.nblk;
   const int g = lane >> 2, t = lane & 3;
@@ -203,16 +203,14 @@ __device__ __forceinline__ void i8_consume(const I8Args &a, const TriItem &it, c
 #pragma unroll
       for (int l = 0; l < I8_LEVELS; ++l) acc[n][l][0][c] = acc[n][l][1][c] = 0;
     }
-  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
   for (int c = 0; c < nch; ++c) {
     const int s = c % I8_STAGES;
-    const int packed = packed_next;
-    if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
     if (*s_fail || !mbar_wait_bounded(smem_addr(&full[s]), (uint32_t)((c / I8_STAGES) & 1))) {
       *s_fail = 1;
       if (lane == 0) atomicOr(a.status, DEV_TIMEOUT);
       return;
     }
+    const int packed = s_packed[s];  // this chunk's layout, written by the producer
     const uint32_t *xs = reinterpret_cast<const uint32_t *>(stages + (size_t)s * a.stage);
     const uint32_t *zs = xs + TRI_CHUNK * px;
     const double2 *ys = reinterpret_cast<const double2 *>(zs + TRI_CHUNK * pz);
@@ -250,6 +248,7 @@ __global__ void __launch_bounds__(32 * (I8_MAX_TILES + 1), I8_MINB) k_triangle_i
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[I8_STAGES], empty[I8_STAGES];
   __shared__ volatile int s_fail;
+  __shared__ volatile int s_packed[I8_STAGES];
   const TriItem it = a.items[blockIdx.x];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ncons = (blockDim.x >> 5) - 1;
@@ -268,15 +267,19 @@ __global__ void __launch_bounds__(32 * (I8_MAX_TILES + 1), I8_MINB) k_triangle_i
   if (warp == ncons) {
     int issued = 0;
     bool failed = false;
-    int packed = 0, y = 0;
-    uint32_t xz = 0;
+    // chunk descriptors are read TRI_META_AHEAD chunks ahead of their copies
+    struct Meta {
+      int packed, y;
+      uint32_t xz;
+    };
     auto meta = [&](int ch) {
       const TriDesc *d = a.descs + ch;
-      packed = d->packed;
-      xz = lane < TRI_CHUNK ? *reinterpret_cast<const uint32_t *>(&d->xz[lane][0]) : 0u;
-      y = d->y[0];
+      return Meta{d->packed, d->y[0], lane < TRI_CHUNK ? *reinterpret_cast<const uint32_t *>(&d->xz[lane][0]) : 0u};
     };
-    if (nch > 0) meta(it.ch0);
+    const Meta none{0, 0, 0u};
+    Meta m0 = nch > 0 ? meta(it.ch0) : none, m1 = nch > 1 ? meta(it.ch0 + 1) : none;
+    Meta m2 = nch > 2 ? meta(it.ch0 + 2) : none, m3 = nch > 3 ? meta(it.ch0 + 3) : none;
+    static_assert(TRI_META_AHEAD == 4, "the descriptor ring below holds four chunks");
     for (int c = 0; c < nch; ++c) {
       const int s = c % I8_STAGES;
       if (c >= I8_STAGES &&
@@ -284,10 +287,13 @@ __global__ void __launch_bounds__(32 * (I8_MAX_TILES + 1), I8_MINB) k_triangle_i
         failed = true;
         break;
       }
-      const int cp = packed, cy = y;
-      const uint32_t cxz = xz;
-      if (c + 1 < nch) meta(it.ch0 + c + 1);
-      i8_issue(a, it, S, smem_raw + (size_t)s * a.stage, smem_addr(&full[s]), cp, cxz, cy);
+      const Meta cur = m0;
+      m0 = m1;
+      m1 = m2;
+      m2 = m3;
+      if (c + TRI_META_AHEAD < nch) m3 = meta(it.ch0 + c + TRI_META_AHEAD);
+      if (lane == 0) s_packed[s] = cur.packed;  // published by i8_issue's arrive on full[s]
+      i8_issue(a, it, S, smem_raw + (size_t)s * a.stage, smem_addr(&full[s]), cur.packed, cur.xz, cur.y);
       issued = c + 1;
     }
     if (failed) {
@@ -301,7 +307,7 @@ __global__ void __launch_bounds__(32 * (I8_MAX_TILES + 1), I8_MINB) k_triangle_i
   }
   // each consumer lane's 8 running sums, 32 lanes apart (after the stages)
   double *sums = reinterpret_cast<double *>(smem_raw + (size_t)I8_STAGES * a.stage) + warp * 8 * 32 + lane;
-  i8_consume(a, it, S, smem_raw, full, empty, &s_fail, warp, lane, nch, real, sums);
+  i8_consume(a, it, S, smem_raw, full, empty, &s_fail, s_packed, warp, lane, nch, real, sums);
 }
 
 int triangle_i8_init_attributes(size_t smem_optin) {

@@ -153,8 +153,8 @@ constexpr int fma_max_cons_warps(int n = 1) {
 // pairs, with the same FP32 operations, in the same order, per combo as below.
 template <typename C>
 __device__ __forceinline__ void tri_consume_fma_tile(const TriArgs &a, const TriItem &it, const C *stages,
-                                                     uint64_t *full, uint64_t *empty, volatile int *s_fail, int warp,
-                                                     int lane, int nch) {
+                                                     uint64_t *full, uint64_t *empty, volatile int *s_fail,
+                                                     const volatile int *s_packed, int warp, int lane, int nch) {
   static_assert(std::is_same<C, float2>::value && TRI_P1 == 8, "the packed consumer is the FP32 path, 8 planes p1");
   const int32_t *tc = a.tile_combo + (size_t)(it.tile0 + warp) * (TRI_P1 * 32) + lane;
   bool any = false;
@@ -170,12 +170,10 @@ __device__ __forceinline__ void tri_consume_fma_tile(const TriArgs &a, const Tri
   unsigned long long wr[TRI_P1 / 2] = {}, wi[TRI_P1 / 2] = {};  // the run's W, planes (2h, 2h+1), across chunks
 #pragma unroll
   for (int q = 0; q < TRI_P1; ++q) sum[q] = 0.0;
-  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
   for (int c = 0; c < nch; ++c) {
     const int s = c % TRI_STAGES;
-    const int packed = packed_next;  // piece layout of this chunk, loaded one chunk ahead
-    if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
     if (!tri_wait_chunk(a, full, s_fail, c, lane)) return;
+    const int packed = s_packed[s];  // piece layout of this chunk, written by the producer
     const float *xs = reinterpret_cast<const float *>(stages + s * a.stage);
     const float *zs = xs + 2 * TRI_CHUNK * it.Lx;
     const float *ys = zs + 2 * TRI_CHUNK * it.Lz;
@@ -247,8 +245,8 @@ __device__ __forceinline__ void tri_consume_fma_tile(const TriArgs &a, const Tri
 // with one plane p3 and 8 planes p1 per lane).
 template <typename C>
 __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem &it, const C *stages, uint64_t *full,
-                                                uint64_t *empty, volatile int *s_fail, int warp, int lane,
-                                                int nch) {
+                                                uint64_t *empty, volatile int *s_fail, const volatile int *s_packed,
+                                                int warp, int lane, int nch) {
   static_assert(std::is_same<C, float2>::value && TRI_P1 == 8 && TRI_BW == 8,
                 "the packed consumer is the FP32 path over 8 x 8 blocks");
   const int j = lane >> 2, ph = (lane >> 1) & 1, vh = lane & 1;
@@ -278,12 +276,10 @@ __device__ __forceinline__ void tri_consume_fma(const TriArgs &a, const TriItem 
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int c = 0; c < 4; ++c) sum[i][c] = 0.0;
-  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
   for (int ch = 0; ch < nch; ++ch) {
     const int s = ch % TRI_STAGES;
-    const int packed = packed_next;  // piece layout of this chunk, loaded one chunk ahead
-    if (ch + 1 < nch) packed_next = a.descs[it.ch0 + ch + 1].packed;
     if (!tri_wait_chunk(a, full, s_fail, ch, lane)) return;
+    const int packed = s_packed[s];  // piece layout of this chunk, written by the producer
     const float *xs = reinterpret_cast<const float *>(stages + s * a.stage);
     const float *zs = xs + 2 * TRI_CHUNK * it.Lx;
     const float *ys = zs + 2 * TRI_CHUNK * it.Lz;
@@ -451,8 +447,8 @@ __device__ __forceinline__ void dmma_pieces(const double2 *xs, const double2 *zs
 // piece each such entry adds Re(y_k2(-p1-p3) * W) to its sum. Per group of
 // four triangles a warp makes 8 128-bit shared loads for 4096 FMA.
 __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem &it, const double2 *stages,
-                                                 uint64_t *full, uint64_t *empty, volatile int *s_fail, int warp,
-                                                 int lane, int nch) {
+                                                 uint64_t *full, uint64_t *empty, volatile int *s_fail,
+                                                 const volatile int *s_packed, int warp, int lane, int nch) {
   static_assert(TRI_P1 == 8, "the DMMA consumer tiles 8 planes p1");
   const TriTile tl = a.tiles[it.tile0 + warp];
   const int nblk = tl.nblk;
@@ -474,12 +470,10 @@ __device__ __forceinline__ void tri_consume_dmma(const TriArgs &a, const TriItem
   double sum[4][2], wr[4][2], wi[4][2];  // wr/wi: the current run's W, carried across chunks
 #pragma unroll
   for (int n = 0; n < 4; ++n) sum[n][0] = sum[n][1] = wr[n][0] = wr[n][1] = wi[n][0] = wi[n][1] = 0.0;
-  int packed_next = nch > 0 ? a.descs[it.ch0].packed : 0;
   for (int c = 0; c < nch; ++c) {
     const int s = c % TRI_STAGES;
-    const int packed = packed_next;
-    if (c + 1 < nch) packed_next = a.descs[it.ch0 + c + 1].packed;
     if (!tri_wait_chunk(a, full, s_fail, c, lane)) return;
+    const int packed = s_packed[s];  // piece layout of this chunk, written by the producer
     const double2 *xs = stages + s * a.stage;
     const double2 *zs = xs + TRI_CHUNK * px;
     const double2 *ys = zs + TRI_CHUNK * pz;
@@ -527,8 +521,8 @@ __host__ __device__ inline int cons_warps(int n) {
 // barriers (empty[] counting ncons arrivals).
 template <typename C>
 __device__ __forceinline__ void tri_run_item(const TriArgs &a, const TriItem &it, unsigned char *smem_raw,
-                                             uint64_t *full, uint64_t *empty, volatile int *s_fail, int producer,
-                                             int ncons) {
+                                             uint64_t *full, uint64_t *empty, volatile int *s_fail,
+                                             volatile int *s_packed, int producer, int ncons) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   C *stages = reinterpret_cast<C *>(smem_raw);
   const C *S = static_cast<const C *>(a.S) + (size_t)a.real * a.s_stride;
@@ -538,7 +532,12 @@ __device__ __forceinline__ void tri_run_item(const TriArgs &a, const TriItem &it
     // ------------------------------------------------------------ producer
     int issued = 0;
     bool failed = false;
-    TriMeta meta = nch > 0 ? tri_meta(a, it.ch0) : TriMeta{0, 0u, 0};
+    // chunk descriptors are read TRI_META_AHEAD chunks ahead of their copies
+    // (they stream from DRAM: one chunk of lookahead left the ring waiting on them)
+    const TriMeta none{0, 0u, 0};
+    TriMeta m0 = nch > 0 ? tri_meta(a, it.ch0) : none, m1 = nch > 1 ? tri_meta(a, it.ch0 + 1) : none;
+    TriMeta m2 = nch > 2 ? tri_meta(a, it.ch0 + 2) : none, m3 = nch > 3 ? tri_meta(a, it.ch0 + 3) : none;
+    static_assert(TRI_META_AHEAD == 4, "the descriptor ring below holds four chunks");
     for (int c = 0; c < nch; ++c) {
       const int s = c % TRI_STAGES;
       if (c >= TRI_STAGES &&
@@ -546,8 +545,12 @@ __device__ __forceinline__ void tri_run_item(const TriArgs &a, const TriItem &it
         failed = true;
         break;
       }
-      const TriMeta cur = meta;
-      if (c + 1 < nch) meta = tri_meta(a, it.ch0 + c + 1);
+      const TriMeta cur = m0;
+      m0 = m1;
+      m1 = m2;
+      m2 = m3;
+      if (c + TRI_META_AHEAD < nch) m3 = tri_meta(a, it.ch0 + c + TRI_META_AHEAD);
+      if (lane == 0) s_packed[s] = cur.packed;  // published by tri_issue's arrive on full[s]
       tri_issue<C>(a, it, S, stages + s * a.stage, smem_addr(&full[s]), cur);
       issued = c + 1;
     }
@@ -565,11 +568,11 @@ __device__ __forceinline__ void tri_run_item(const TriArgs &a, const TriItem &it
 
   // -------------------------------------------------------------- consumer
   if constexpr (std::is_same<C, double2>::value)
-    tri_consume_dmma(a, it, stages, full, empty, s_fail, warp, lane, nch);
+    tri_consume_dmma(a, it, stages, full, empty, s_fail, s_packed, warp, lane, nch);
   else if (!fma_pairs_tiles(it.ntiles))
-    tri_consume_fma_tile<C>(a, it, stages, full, empty, s_fail, warp, lane, nch);
+    tri_consume_fma_tile<C>(a, it, stages, full, empty, s_fail, s_packed, warp, lane, nch);
   else
-    tri_consume_fma<C>(a, it, stages, full, empty, s_fail, warp, lane, nch);
+    tri_consume_fma<C>(a, it, stages, full, empty, s_fail, s_packed, warp, lane, nch);
 }
 
 // One CTA per item of one tile class (blockIdx.x) and realization (blockIdx.y);
@@ -579,6 +582,7 @@ __global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks) k
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[TRI_STAGES], empty[TRI_STAGES];
   __shared__ volatile int s_fail;
+  __shared__ volatile int s_packed[TRI_STAGES];
   const TriItem it = a.items[blockIdx.x];
   const int tid = threadIdx.x;
   const int ncons = (blockDim.x >> 5) - 1;  // consumer warps (cons_warps); warp ncons produces
@@ -593,7 +597,7 @@ __global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks) k
   __syncthreads();
   TriArgs b = a;
   b.real = blockIdx.y;
-  tri_run_item<C>(b, it, smem_raw, full, empty, &s_fail, ncons, ncons);
+  tri_run_item<C>(b, it, smem_raw, full, empty, &s_fail, s_packed, ncons, ncons);
 }
 
 // Persistent form: every item of every tile class and every realization in one
@@ -608,6 +612,7 @@ __global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t full[TRI_STAGES], empty[TRI_STAGES];
   __shared__ volatile int s_fail;
+  __shared__ volatile int s_packed[TRI_STAGES];
   __shared__ int s_unit;
   const int tid = threadIdx.x;
   const int producer = (blockDim.x >> 5) - 1;
@@ -636,7 +641,7 @@ __global__ void __launch_bounds__(TriBounds<C>::threads, TriBounds<C>::blocks)
     TriArgs b = a;
     b.real = w % a.nreal;
     b.stage = a.stage_of[it.ntiles];
-    tri_run_item<C>(b, it, smem_raw, full, empty, &s_fail, producer, ncons);
+    tri_run_item<C>(b, it, smem_raw, full, empty, &s_fail, s_packed, producer, ncons);
   }
 }
 
