@@ -12,7 +12,7 @@
  * The reference's hard-coded constants (barbie.c:67-84) are the defaults;
  * optional environment overrides, all unset by default:
  *   BEAM_NMAX, BEAM_NR        planes and rings (100, 40)
- *   BEAM_PRECISION            fp64 (default) or mixed
+ *   BEAM_PRECISION            fp64 (default), mixed (FP32) or int8 (exact 8-bit slice products)
  *   BEAM_METHOD               triangle (default) or pixel
  *   BEAM_DEVICE               CUDA device ordinal (0)
  *   BEAM_PRINT_DIGITS         significant digits of columns 4-6 (default: the
@@ -68,6 +68,7 @@ int main(int argc, char *argv[]) {
   cfg.Nr = env_long("BEAM_NR", cfg.Nr);
   const char *prec = getenv("BEAM_PRECISION");
   if (prec && strcmp(prec, "mixed") == 0) cfg.precision = BEAM_PREC_MIXED;
+  if (prec && strcmp(prec, "int8") == 0) cfg.precision = BEAM_PREC_INT8;
   const char *meth = getenv("BEAM_METHOD");
   if (meth && strcmp(meth, "pixel") == 0) cfg.method = BEAM_METHOD_PIXEL;
   int digits = (int)env_long("BEAM_PRINT_DIGITS", 0);
