@@ -86,3 +86,27 @@ def test_int8_cubic_scaling(beamlib, ctx):
     assert np.array_equal(b["count"], a["count"])
     assert np.array_equal(b["norm"], a["norm"])
     assert np.array_equal(b["out"], 8.0 * a["out"], equal_nan=True)
+
+
+@pytest.mark.parametrize("shards", [2, 3])
+def test_int8_shard_partials_add_up(beamlib, ctx, shards):
+    """A bispectrum split by ring triplet over shards: each shard's int8 plan
+    sums its own triplets (the others' triangles enter as exact zeros), and
+    the partial bins add up to the unsharded int8 run up to the rounding of
+    the final additions."""
+    from barbie_b200 import shard
+    case = GOLDEN_CASES["nn96_r20"]
+    f = golden_field("nn96_r20")
+    whole_plan = make_plan(beamlib, ctx, case, precision="int8")
+    whole = whole_plan.run(f)
+    parts = []
+    for k in range(shards):
+        p = make_plan(beamlib, ctx, case, precision="int8", shard=(k, shards))
+        parts.append(p.run(f))
+        p.close()
+    got = shard.sum_partials(parts, whole_plan.info["vol"])
+    whole_plan.close()
+    assert np.array_equal(got["count"], whole["count"])
+    for key in ("bs", "norm"):
+        scale = np.maximum(np.abs(whole[key]), sum(np.abs(p[key]) for p in parts))
+        assert np.all(np.abs(got[key] - whole[key]) <= 1e-12 * scale), key

@@ -40,7 +40,7 @@ def assert_same(got, want):
 
 
 MIX = [("nn96_r20", "fp64"), ("nn256_cfg2", "fp64"), ("nn96_r20", "mixed"), ("nn64_bw2", "fp64"),
-       ("nn64_cfg1", "fp64")]
+       ("nn64_cfg1", "fp64"), ("nn96_r20", "int8")]
 
 
 def test_jobs_give_the_same_bins_alone_and_in_the_mix(beamlib, ctx):
