@@ -401,7 +401,9 @@ void gather_host(const beam_gpu_plan *p, RunSlot *s, int r, const double *r2c, i
 int upload_modes(beam_gpu_plan *p, RunSlot *s, int n, bool staged, bool staged_on_device = false);
 int gather_mapped(beam_gpu_plan *p, RunSlot *s, const double *r2c_mapped);
 int run_triangle_sums(beam_gpu_plan *p, RunSlot *s, int n);
-// int8 path (beam_tri_i8.cu)
+// int8 path: slice tables of realizations [0, n) from their FP64 rows (beam_run.cu); the
+// triangle sums (beam_tri_i8.cu)
+int build_slices(beam_gpu_plan *p, RunSlot *s, int n);
 int launch_triangle_i8(beam_gpu_plan *p, RunSlot *s, int nreal);
 int triangle_i8_init_attributes(size_t smem_optin);
 int run_epilogue(beam_gpu_plan *p, RunSlot *s, int n);

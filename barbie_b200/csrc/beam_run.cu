@@ -152,7 +152,7 @@ __global__ void k_build_slices(const double2 *__restrict__ S, long long real_str
 }
 
 // Scales and slice rows of realizations [0, n) from their FP64 rows.
-static int build_slices(beam_gpu_plan *p, RunSlot *s, int n) {
+int build_slices(beam_gpu_plan *p, RunSlot *s, int n) {
   const DevPlan &d = p->d;
   cudaStream_t st = s->lane->stream;
   const long long real_bytes = (long long)mode_data_bytes(d);

@@ -84,11 +84,12 @@ static int time_triangle_phase(beam_gpu_plan *p, int reps, float *best) {
   RunSlot *s = p->main;
   cudaStream_t st = p->ctx->stream;
   const size_t n = (size_t)p->d.n_modes * p->d.W * 2;  // real values of one realization's S
-  if (p->d.elem == sizeof(double2))
-    k_fill_pattern<<<4 * p->ctx->num_sms, 256, 0, st>>>((double *)s->S, n);
-  else
+  if (p->d.elem == sizeof(float2))
     k_fill_pattern_f<<<4 * p->ctx->num_sms, 256, 0, st>>>((float *)s->S, n);
+  else  // FP64 rows (the int8 path's come first, its slice tables are cut from them)
+    k_fill_pattern<<<4 * p->ctx->num_sms, 256, 0, st>>>((double *)s->S, n);
   BEAM_CUDA(cudaGetLastError());
+  if (p->d.i8) BEAM_TRY(build_slices(p, s, 1));
   cudaEvent_t e0, e1;
   BEAM_CUDA(cudaEventCreate(&e0));
   BEAM_CUDA(cudaEventCreate(&e1));

@@ -681,6 +681,46 @@ def cpu_baseline_port(field, info):
 
 
 # --------------------------------------------------------------- reference
+def reference_full_run_check(ref_bin, cores):
+    """A whole reference run at a small configuration (barbie 96 1 21 1 1 with
+    Nmax=32, Nr=20), timed, beside the per-triangle extrapolation the arm uses
+    at NN=384 applied to the same configuration (windows of ring triplets of
+    one p1, one process at a time): how far the extrapolated triangle-loop
+    time is from the measured one."""
+    from oracle import oracle_py
+    from barbie_b200.synth import realization_seed, synth_field, write_field
+    NN, Nmax, Nr, UL, LL, BW = 96, 32, 20, 21, 1, 1
+    scratch = tempfile.mkdtemp(prefix="beam_refcheck_")
+    try:
+        os.makedirs(os.path.join(scratch, f"ResFiles_N{NN}", "data_files"), exist_ok=True)
+        write_field(os.path.join(scratch, f"field_N{NN}_R1.txt"), synth_field(NN, realization_seed(1)))
+        env = dict(os.environ, BEAM_REF_NMAX=str(Nmax), BEAM_REF_NR=str(Nr), BEAM_REF_NTHREADS=str(cores))
+
+        def run(extra):
+            out = subprocess.run(["bash", "-c", f"ulimit -s unlimited; exec {ref_bin} {NN} 1 {UL} {LL} {BW}"],
+                                 cwd=scratch, env=dict(env, **extra), capture_output=True, text=True)
+            m = re.search(r"Total time ([0-9.]+)", out.stdout)
+            return float(m.group(1)) if m else None
+
+        full = run({})  # builds the caches, then the whole triangle loop
+        rings = oracle_py.closed_rings(NN, Nr, Nmax)
+        tri, _ = oracle_py.enumerate_triples(NN, Nmax, Nr, UL, LL, BW, rings4=rings)
+        per_tri = []
+        for p1 in sorted(set(int(v) for v in tri["p1"]))[::4]:
+            counts = np.bincount(tri["rp"][tri["p1"] == p1], minlength=len(rings))
+            n = int(counts.sum())
+            t = run({"BEAM_REF_P1_LO": str(p1), "BEAM_REF_P1_HI": str(p1 + 1)}) if n else None
+            if t and t > 0:
+                per_tri.append(t / n)
+        pred = len(tri) * float(np.median(per_tri)) if per_tri else None
+        return {"workload": f"barbie {NN} 1 {UL} {LL} {BW}, Nmax={Nmax}, Nr={Nr}", "triangles": int(len(tri)),
+                "measured_loop_s": full, "extrapolated_loop_s": pred,
+                "extrapolated_over_measured": (pred / full) if (pred and full) else None,
+                "samples": f"{len(per_tri)} single-p1 runs, one process at a time"}
+    finally:
+        shutil.rmtree(scratch, ignore_errors=True)
+
+
 def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
@@ -782,6 +822,10 @@ def run_reference(args):
                                               "seconds_per_bispectrum": ntri * float(np.median(per_tri)) + t_cache + t_calcr}
                                              if per_tri else None)},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        line["cpu_baseline"]["full_run_check"] = reference_full_run_check(ref_bin, cores)
+    except (OSError, subprocess.SubprocessError, ValueError) as e:
+        line["cpu_baseline"]["full_run_check"] = {"error": str(e)}
     print(json.dumps(line), flush=True)
     shutil.rmtree(scratch, ignore_errors=True)  # the reference's disk caches: ~9.4 GB at NN=384
 
