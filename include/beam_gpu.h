@@ -59,7 +59,9 @@ extern "C" {
 #define BEAM_PREC_MIXED 1 /* FP32 mode data and products, FP32 chunk sums, FP64 across chunks */
 #define BEAM_PREC_INT8 2  /* FP64 mode data cut into five 8-bit slices per (ring, plane) scale; the
                              slice products and each run's sums exact in int32 on the int8 tensor
-                             cores; FP64 from the run's end on (error ~1e-7 of a bin, far below 1e-5) */
+                             cores; FP64 from the run's end on (error ~1e-7 of a bin, far below 1e-5).
+                             Mode values must be finite: a NaN or infinity is not carried through the
+                             slices as the FP64 path carries it */
 
 /* how the per-triangle sums B = sum_x Re(F1 F2 F3) are formed */
 #define BEAM_METHOD_TRIANGLE 0 /* over closed in-plane Fourier triangles (default) */
